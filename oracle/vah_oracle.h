@@ -1,0 +1,62 @@
+/*
+ * oracle/vah_oracle.h -- test infrastructure: the CPU checker's API.
+ *
+ * A plain-C restatement of the reference CPU time step
+ * (old_cpu-vah_code/src, driven as rhic/src/HydroPlugin.cpp:208-233 drives the
+ * GPU build). Only tests, the smoke check and the CPU-baseline leg of the
+ * benchmark load it; the product never does.
+ *
+ * Physics variants are chosen at run time instead of the reference's macros:
+ *   VO_IDEAL      N_q = 5  (no PIMUNU, no PI: the CPU header's default)
+ *   VO_PIMUNU     N_q = 15 (-DPIMUNU)
+ *   VO_PIMUNU_PI  N_q = 16 (-DPIMUNU -DPI)
+ * W^mu_{perp z} (W_TZ_MU) is off in every reference build and not restated.
+ *
+ * Arrays use the reference layout: field[i + ncx*(j + ncy*k)] with
+ * nc = n + 4 (2 ghost layers per side), DynamicalVariables.cpp:29-31.
+ */
+#ifndef VAH_ORACLE_H
+#define VAH_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { VO_IDEAL = 0, VO_PIMUNU = 1, VO_PIMUNU_PI = 2 };
+enum { VO_EOS_CONFORMAL = 0, VO_EOS_TABLE = 1 };
+enum { VO_ZETA_REFERENCE = 0, VO_ZETA_CROSSOVER = 1 };
+
+typedef struct {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double etabar;            /* eta/s */
+    int physics;              /* VO_IDEAL / VO_PIMUNU / VO_PIMUNU_PI */
+    int eos;                  /* VO_EOS_* */
+    int zeta;                 /* VO_ZETA_* */
+    const double *eos_table;  /* VO_EOS_TABLE only; layout in vo_eos.h */
+} vo_config;
+
+typedef struct vo_state vo_state;
+
+vo_state *vo_create(const vo_config *cfg);
+void vo_destroy(vo_state *st);
+int vo_num_cells(const vo_state *st);      /* ncx*ncy*ncz */
+double *vo_field(vo_state *st, int id);    /* ids as include/vah.h VAH_F_* */
+void vo_set_conserved(vo_state *st, double t, int pl_from_field);
+void vo_set_ghost_cells(vo_state *st);
+void vo_step(vo_state *st, double t, double dt);
+double vo_run(vo_state *st, double t0, double dt, int nsteps);
+/* counts of inversion fallbacks / NaNs seen during the last step:
+ * out[0] face (flux) fallbacks, out[1] cell fallbacks, out[2] NaNs */
+void vo_last_step_stats(const vo_state *st, long long out[3]);
+
+/* Single-cell operators, for unit tests of the library's pieces. */
+int vo_infer(const vo_config *cfg, double t, const double *q, double ePrev, double uT0,
+             double *out /* e, p, ut, ux, uy, un */);
+double vo_approx_derivative(double qm, double q, double qp);
+void vo_eos_eval(const vo_config *cfg, double e, double *out /* p, T, cs2 */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
