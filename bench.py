@@ -1,0 +1,350 @@
+"""Benchmark of the VAH time step on B200.
+
+Workload: one 3+1D MC-Glauber Au+Au event (b = 7 fm) on a 121x121x81 grid,
+dx = dy = 0.1 fm, d(eta) = 0.1, tabulated crossover EoS, eta/s = 0.16,
+crossover zeta/s, shear + bulk (N_q = 16), FP64, tau0 = 0.25 fm/c,
+d(tau) = 0.005 fm/c. A step is one Heun RK2 step of the whole grid; the
+metric is interior cell-updates per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank advances its own event (seed 1 + rank): events are
+independent, so multi-GPU is replicas with weak scaling and no data-path
+collective. Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-vah_b200"))
+
+NX, NY, NZ = 121, 121, 81
+DX, DZ = 0.1, 0.1
+T0, DT, ETA_S = 0.25, 0.005, 0.16
+B_IMPACT = 7.0
+NQ = 16
+BYTES_PER_CELL_UPDATE = (5 * NQ + 32) * 8  # algorithmic HBM bytes, FP64 storage
+WORKLOAD = "vah 3+1D MC-Glauber Au+Au b=7fm 121x121x81 dx=0.1 deta=0.1 table-EoS shear+bulk FP64"
+SAMPLE_NZ = 5  # eta slices of the CPU sample slab
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="vah", choices=["vah", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def initial_energy_density(vah, table, seed, nx=NX, ny=NY, nz=NZ):
+    """MC-Glauber transverse profile x plateau+Gaussian longitudinal profile,
+    peak temperature 0.6 GeV under the tabulated EoS (interior, x fastest)."""
+    e_peak = vah.table_energy_density(table, 0.6 / vah.HBARC)
+    exy, _ = vah.mc_glauber(nx, ny, DX, DX, B_IMPACT, seed, e_peak=e_peak)
+    f = vah.longitudinal(NZ, DZ)
+    k0 = (NZ - nz) // 2
+    return np.ascontiguousarray((f[k0:k0 + nz, None] * exy[None, :]).ravel())
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                                 parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU baseline --
+def _ref_worker(args):
+    """Run the reference's own CPU step (oracle/_ref) on the sample slab."""
+    conn, steps, warm, seed = args
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import vahlib as V
+    table = V.eos_table()
+    g = V.Grid(NX, NY, SAMPLE_NZ, DX, DX, DZ, ETA_S, physics="pimunu_pi", eos="table", zeta="crossover",
+               table=table)
+    use_ref = V.ref_available(g.physics, g.eos)
+    impl = V.Reference(g) if use_ref else V.Oracle(g)
+    e = initial_energy_density(V.product, table, seed, NX, NY, SAMPLE_NZ).reshape(SAMPLE_NZ, NY, NX)
+    full = np.zeros(g.shape)
+    full[2:-2, 2:-2, 2:-2] = e
+    p = np.interp(np.log(np.maximum(full, 1e-300)), table[1] + table[3] * np.arange(int(table[0])),
+                  table[8:8 + int(table[0])])
+    V.load_state(impl, {V.E: full.ravel(), V.PP: p.ravel(), V.UT: np.ones(g.ncell), V.PL: p.ravel()})
+    if use_ref:
+        impl.set_conserved(T0)  # the reference's own initialisation
+    else:
+        impl.set_conserved(T0, 0)
+    impl.set_ghost_cells()
+    conn.send(("ready", "reference" if use_ref else "port"))
+    t = T0
+    for n in range(warm + steps):
+        conn.recv()
+        a = time.perf_counter()
+        impl.step(t, DT)
+        conn.send(time.perf_counter() - a)
+        t += DT
+    conn.close()
+
+
+def cpu_step_rate(workers, steps, warmup, seed=1):
+    """Spawned workers (one per host core used) step their own copy of the
+    sample slab in lockstep; returns (cell-updates/s, kind, per-step wall s)."""
+    ctx = mp.get_context("spawn")
+    pipes, procs = [], []
+    for w in range(workers):
+        a, b = ctx.Pipe()
+        p = ctx.Process(target=_ref_worker, args=((b, steps, warmup, seed + w),))
+        p.start()
+        pipes.append(a)
+        procs.append(p)
+    kinds = {pipe.recv()[1] for pipe in pipes}
+    walls = []
+    for n in range(warmup + steps):
+        a = time.perf_counter()
+        for pipe in pipes:
+            pipe.send("go")
+        for pipe in pipes:
+            pipe.recv()
+        if n >= warmup:
+            walls.append(time.perf_counter() - a)
+    for p in procs:
+        p.join(timeout=60)
+    cells = NX * NY * SAMPLE_NZ
+    rate = workers * cells * len(walls) / sum(walls)
+    return rate, kinds.pop(), walls
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# -------------------------------------------------------------- main arms --
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    workers = max(1, min(host_cores(), 64))
+    rate, kind, walls = cpu_step_rate(workers, args.steps, args.warmup)
+    ms = 1000 * statistics.mean(walls)
+    sample = f"{NX}x{NY}x{SAMPLE_NZ} central-eta slab of the workload per worker, one RK2 step per worker per step"
+    line = {"impl": "reference", "metric": "cell-updates/s", "value": rate, "unit": "cell-updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": NX * NY * NZ, "global_batch": 1, "parallelism": "replicas"},
+            "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": workers, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def traffic_per_launch(cells):
+    """DRAM bytes of one stage-kernel launch from the committed ncu summary
+    (bytes per interior cell, scaled to this launch), or None."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_dram.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get("dram_bytes_per_cell_per_launch", 0) * cells or None
+
+
+def run_vah(args, rank, world, dist):
+    import torch
+    import vah
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()  # a real stream handle: the library queues its kernels on it
+    table = vah.eos_table()
+    e0 = initial_energy_density(vah, table, seed=1 + rank)
+    ev = vah.Event(NX, NY, NZ, DX, DX, DZ, ETA_S, physics=vah.VAH_PIMUNU_PI, eos=vah.VAH_EOS_TABLE,
+                   zeta=vah.VAH_ZETA_CROSSOVER, table=table, t0=T0, device=local, stream=stream.cuda_stream)
+    ev.init_from_e(T0, e0, vah.VAH_PL_ISOTROPIC)
+    t = T0
+    ev.run(t, DT, args.warmup)
+    t += args.warmup * DT
+    ev.sync()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    ev.set_timing(True)
+    ev.kernel_time()  # reset
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        start.record(stream)
+        ev.run(t, DT, args.steps)
+        end.record(stream)
+        torch.cuda.synchronize()
+    t += args.steps * DT
+    elapsed = start.elapsed_time(end) / 1000.0
+    kms, launches = ev.kernel_time()
+    ev.set_timing(False)
+    ev.sync()
+    if dist is not None:
+        tt = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    cells = NX * NY * NZ
+    value = world * cells * args.steps / elapsed
+
+    # end to end through the host-buffer entry point (pinned host state, H2D + step + D2H per step)
+    ids = list(range(16)) + list(range(16, 26))
+    host = {fid: torch.from_numpy(ev.get_field(fid)).pin_memory() for fid in ids}
+    ptrs = [host[fid].data_ptr() if fid in host else 0 for fid in range(vah.NUM_FIELDS)]
+    ev.step_host(t, DT, ptrs)  # warm
+    t += DT
+    barrier()
+    a = time.perf_counter()
+    for n in range(args.e2e_steps):
+        ev.step_host(t, DT, ptrs)
+        t += DT
+    e2e_s = time.perf_counter() - a
+    if dist is not None:
+        tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_value = world * cells * args.e2e_steps / e2e_s
+    state_bytes = sum(h.numel() * 8 for h in host.values())
+    stats = ev.stats()
+    ev.close()
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    avg_launch_s = kms / 1000.0 / max(launches, 1)
+    bytes_per_launch = BYTES_PER_CELL_UPDATE / 2 * cells
+    achieved = bytes_per_launch / avg_launch_s / 1e9
+    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": cells, "global_batch": world, "parallelism": "replicas",
+                       "l2": "inputs larger than L2 (state 0.55 GB per event)", "dt_fm": DT, "tau0_fm": T0},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic_per_launch(cells),
+                         "peak_kind": f"{peak_kind} copy bandwidth",
+                         "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
+                         "kernel": "stage_kernel (one fused RK stage), average of the two stage launches",
+                         "avg_launch_ms": 1000 * avg_launch_s},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
+                    "path": "vah_rk2_step_host (pinned host state in, one step, state out)"},
+            "gpu_launches": launches,
+            "stats": {"face_fallbacks": stats.face_fallbacks, "cell_fallbacks": stats.cell_fallbacks,
+                      "nan_cells": stats.nan_cells}}
+    clk_summary = clk.summary()
+    if clk_summary:
+        line["clocks"] = clk_summary
+    if world == 1 and not args.no_cpu_baseline:
+        rate, kind, walls = cpu_step_rate(1, 2, 0)
+        line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": 1, "kind": kind,
+                                "sample": f"{NX}x{NY}x{SAMPLE_NZ} central-eta slab of the workload, 2 RK2 steps"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+        if args.impl == "reference":
+            if rank != 0:
+                return
+        else:
+            dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            dist = dist_mod
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_vah(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+// vah_kernels.cu -- CUDA kernels of the VAH time step (sm_100a).
+//
+// stage_kernel: one thread per interior cell runs the whole RK stage of that
+// cell (vah_stage.cuh). The step is FP64-arithmetic-bound (13 Newton
+// inversions per cell and stage in the reference-faithful flux mode), so the
+// launch favours occupancy: 128-thread blocks shaped 32 (x) by 4 (y*z rows),
+// x fastest so that every load of a field is a coalesced 32-wide row.
+#include "vah_kernels.cuh"
+
+namespace vah {
+
+namespace {
+
+constexpr int kBX = 32, kBY = 4;
+
+template <typename S, int PHYS, bool IS3D>
+__global__ void __launch_bounds__(kBX *kBY) stage_kernel(const StageArgs<S> a) {
+    const int i = blockIdx.x * kBX + threadIdx.x;
+    const int r = blockIdx.y * kBY + threadIdx.y;  // row index over (j, k)
+    if (i >= a.nx || r >= a.ny * a.nz) return;
+    const int j = r % a.ny, k = r / a.ny;
+    stage_cell<S, PHYS, IS3D>(a, i + 2, j + 2, k + 2);
+}
+
+template <typename S, int PHYS>
+__global__ void set_conserved_kernel(const FieldSet<S> q, const FieldSet<S> u, const FieldSet<S> up, const S *e,
+                                     int nx, int ny, int nz, double t, int pl_from_field) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+        const long long s = (i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * (k + 2));
+        set_conserved_cell<S, PHYS>(q.f, u.f, up.f, e, t, pl_from_field, s);
+    }
+}
+
+template <typename S>
+__global__ void init_primitives_kernel(const FieldSet<S> q, const FieldSet<S> u, const S *e, S *p, const Eos eos,
+                                       int nx, int ny, int nz) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+        const long long s = (i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * (k + 2));
+        const double pv = eos_pressure(eos, (double)e[s]);
+        p[s] = (S)pv;
+        u.f[0][s] = (S)1.0;
+        u.f[1][s] = u.f[2][s] = u.f[3][s] = (S)0.0;
+        for (int m = 5; m < 16; ++m)
+            if (q.f[m]) q.f[m][s] = (S)0.0;
+        q.f[kSlotPL][s] = (S)pv;
+    }
+}
+
+// Pass 0 (I): j in [2, ncy), k in [2, ncz): i = 0,1 <- 2; i = nx+2, nx+3 <- nx+1.
+// Pass 1 (J): i in [2, ncx), k in [2, ncz).  Pass 2 (K): i in [2, ncx), j in [2, ncy).
+template <typename S>
+__global__ void ghost_kernel(const FieldSet<S> f, int nx, int ny, int nz, int pass) {
+    const int ncx = nx + 4, ncy = ny + 4, ncz = nz + 4;
+    const long long plane = (long long)ncx * ncy;
+    int na, nb;
+    if (pass == 0) { na = ncy - 2; nb = ncz - 2; }
+    else if (pass == 1) { na = ncx - 2; nb = ncz - 2; }
+    else { na = ncx - 2; nb = ncy - 2; }
+    const long long n = (long long)na * nb * 4;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int slot = (int)(c & 3);
+        const long long ab = c >> 2;
+        const int A = (int)(ab % na) + 2, B = (int)(ab / na) + 2;
+        long long s, sb;
+        if (pass == 0) {
+            int gi = slot < 2 ? slot : nx + slot, bi = slot < 2 ? 2 : nx + 1;
+            s = gi + (long long)ncx * A + plane * B;
+            sb = bi + (long long)ncx * A + plane * B;
+        } else if (pass == 1) {
+            int gj = slot < 2 ? slot : ny + slot, bj = slot < 2 ? 2 : ny + 1;
+            s = A + (long long)ncx * gj + plane * B;
+            sb = A + (long long)ncx * bj + plane * B;
+        } else {
+            int gk = slot < 2 ? slot : nz + slot, bk = slot < 2 ? 2 : nz + 1;
+            s = A + (long long)ncx * B + plane * gk;
+            sb = A + (long long)ncx * B + plane * bk;
+        }
+        for (int m = 0; m < f.n; ++m) f.f[m][s] = f.f[m][sb];
+    }
+}
+
+template <typename S, int PHYS>
+cudaError_t stage_dispatch(const StageArgs<S> &a, cudaStream_t stream) {
+    dim3 block(kBX, kBY);
+    dim3 grid((a.nx + kBX - 1) / kBX, (a.ny * a.nz + kBY - 1) / kBY);
+    if (a.nz > 1)
+        stage_kernel<S, PHYS, true><<<grid, block, 0, stream>>>(a);
+    else
+        stage_kernel<S, PHYS, false><<<grid, block, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+int grid_for(long long n, int block) {
+    long long g = (n + block - 1) / block;
+    if (g > 148 * 64) g = 148 * 64;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+}  // namespace
+
+template <typename S>
+cudaError_t launch_stage(const StageArgs<S> &a, int physics, cudaStream_t stream) {
+    switch (physics) {
+    case kIdeal: return stage_dispatch<S, kIdeal>(a, stream);
+    case kPimunu: return stage_dispatch<S, kPimunu>(a, stream);
+    case kPimunuPi: return stage_dispatch<S, kPimunuPi>(a, stream);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename S>
+cudaError_t launch_set_conserved(const FieldSet<S> &q, const FieldSet<S> &u, const FieldSet<S> &up, const S *e,
+                                 int physics, int nx, int ny, int nz, double t, int pl_from_field,
+                                 cudaStream_t stream) {
+    const int block = 256;
+    const int grid = grid_for((long long)nx * ny * nz, block);
+    switch (physics) {
+    case kIdeal: set_conserved_kernel<S, kIdeal><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, t, pl_from_field); break;
+    case kPimunu: set_conserved_kernel<S, kPimunu><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, t, pl_from_field); break;
+    case kPimunuPi: set_conserved_kernel<S, kPimunuPi><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, t, pl_from_field); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename S>
+cudaError_t launch_init_primitives(const FieldSet<S> &q, const FieldSet<S> &u, const S *e, S *p, const Eos &eos,
+                                   int nx, int ny, int nz, cudaStream_t stream) {
+    const int block = 256;
+    init_primitives_kernel<S><<<grid_for((long long)nx * ny * nz, block), block, 0, stream>>>(q, u, e, p, eos, nx, ny,
+                                                                                                nz);
+    return cudaGetLastError();
+}
+
+template <typename S>
+cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cudaStream_t stream) {
+    const int block = 256;
+    for (int pass = 0; pass < 3; ++pass) {
+        long long n;
+        if (pass == 0) n = (long long)ny * nz;
+        else if (pass == 1) n = (long long)nx * nz;
+        else n = (long long)nx * ny;
+        n = (n + 4LL * (nx + ny + nz) + 16) * 4;  // the passes also sweep upper ghost rows
+        ghost_kernel<S><<<grid_for(n, block), block, 0, stream>>>(fields, nx, ny, nz, pass);
+        cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
+    }
+    return cudaSuccess;
+}
+
+template cudaError_t launch_stage<double>(const StageArgs<double> &, int, cudaStream_t);
+template cudaError_t launch_set_conserved<double>(const FieldSet<double> &, const FieldSet<double> &,
+                                                  const FieldSet<double> &, const double *, int, int, int, int,
+                                                  double, int, cudaStream_t);
+template cudaError_t launch_init_primitives<double>(const FieldSet<double> &, const FieldSet<double> &,
+                                                    const double *, double *, const Eos &, int, int, int,
+                                                    cudaStream_t);
+template cudaError_t launch_ghosts<double>(const FieldSet<double> &, int, int, int, cudaStream_t);
+
+}  // namespace vah

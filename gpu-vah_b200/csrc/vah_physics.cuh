@@ -1,0 +1,637 @@
+// vah_physics.cuh -- per-cell physics of the VAH time step.
+//
+// Everything here is __host__ __device__: the CUDA kernels (vah_kernels.cu)
+// call it per thread, and the same code builds for the host so its formulas
+// can be checked against the CPU oracle without a GPU. Arithmetic follows the
+// reference CPU path (old_cpu-vah_code/src); where a cheaper but equivalent
+// form is used (reciprocal square roots, v*q instead of u*q/ut, no W terms),
+// results move by rounding only.
+#pragma once
+
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#ifdef __CUDACC__
+#define VAH_HD __host__ __device__ __forceinline__
+#else
+#define VAH_HD inline
+#endif
+
+#include "vah_closure_polys.h"
+
+namespace vah {
+
+constexpr int kIdeal = 0, kPimunu = 1, kPimunuPi = 2;
+
+template <int PHYS>
+struct Phys {
+    static constexpr int NQ = PHYS == kIdeal ? 5 : (PHYS == kPimunu ? 15 : 16);
+    static constexpr bool PIMUNU = PHYS != kIdeal;
+    static constexpr bool BULK = PHYS == kPimunuPi;
+};
+
+constexpr int kSlotPL = 4;
+constexpr int kSlotPi = 15;
+constexpr double kEosFactor = 13.8997;  // EquationOfState.h:16
+constexpr double kHbarc = 0.197326938;
+
+// ------------------------------------------------------------ math helpers --
+VAH_HD double rsqrt_d(double x) {
+#ifdef __CUDA_ARCH__
+    return rsqrt(x);
+#else
+    return 1.0 / sqrt(x);
+#endif
+}
+
+VAH_HD uint32_t float_bits(float x) {
+#ifdef __CUDA_ARCH__
+    return __float_as_uint(x);
+#else
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    return u;
+#endif
+}
+
+template <typename T>
+VAH_HD T ldg(const T *p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
+// ------------------------------------------------------------------- EoS --
+// Equation of state and zeta/s, passed by value into kernels.
+struct Eos {
+    int kind;               // 0: conformal (reference quirks), 1: table
+    int zeta;               // 0: reference zeta/s, 1: crossover zeta/s
+    const double *tab;      // table (layout in include/vah.h)
+    const uint32_t *exc;    // conformal T: (input, result) pairs where the
+    int nexc;               //   reference libm's powf(x, 0.25f) is not the
+                            //   correctly rounded value (see vah_powf_exc.cpp)
+};
+
+// Conformal T = powf(e/13.8997, 0.25) in single precision
+// (EquationOfState.cpp:144). The fourth root is taken in double and rounded
+// once, which gives the correctly rounded single; the reference's libm powf
+// differs from that for a small set of inputs, listed in eos.exc as
+// (input bits, libm result bits) pairs sorted by input (vah_powf_exc.cpp).
+VAH_HD double conformal_T(const Eos &eos, double e) {
+    float xf = (float)(e / kEosFactor);
+    float r = (float)sqrt(sqrt((double)xf));
+    if (eos.nexc > 0) {
+        uint32_t key = float_bits(xf);
+        int lo = 0, hi = eos.nexc - 1;
+        while (lo <= hi) {
+            int mid = (lo + hi) >> 1;
+            uint32_t v = ldg(eos.exc + 2 * mid);
+            if (v == key) {
+                uint32_t rb = ldg(eos.exc + 2 * mid + 1);
+                memcpy(&r, &rb, 4);
+                break;
+            }
+            if (v < key) lo = mid + 1; else hi = mid - 1;
+        }
+    }
+    return (double)r;
+}
+
+struct EosPoint {
+    double p, T, cs2;
+};
+
+// Tabulated EoS: linear interpolation in ln e between nodes; power-law
+// continuation outside (p/e and c_s^2 frozen, T ~ e^(3/23) below, e^(1/4) above).
+template <bool NEED_P, bool NEED_TC>
+VAH_HD EosPoint table_lookup(const double *tab, double e) {
+    EosPoint r{0.0, 0.0, 0.0};
+    const int n = (int)ldg(tab);
+    const double *P = tab + 8, *T = P + n, *C = T + n;
+    if (!(e > 0.0)) {
+        if (NEED_P) r.p = e * (ldg(P) / ldg(tab + 4));
+        if (NEED_TC) r.cs2 = ldg(C);
+        return r;
+    }
+    const double x = log(e);
+    const double f = (x - ldg(tab + 1)) * ldg(tab + 2);
+    if (f <= 0.0) {
+        if (NEED_P) r.p = e * (ldg(P) / ldg(tab + 4));
+        if (NEED_TC) {
+            r.T = ldg(T) * exp((3.0 / 23.0) * (x - ldg(tab + 1)));
+            r.cs2 = ldg(C);
+        }
+        return r;
+    }
+    if (f >= (double)(n - 1)) {
+        if (NEED_P) r.p = e * (ldg(P + n - 1) / ldg(tab + 6));
+        if (NEED_TC) {
+            r.T = ldg(T + n - 1) * exp(0.25 * (x - ldg(tab + 5)));
+            r.cs2 = ldg(C + n - 1);
+        }
+        return r;
+    }
+    const int i = (int)f;
+    const double w = f - (double)i;
+    if (NEED_P) {
+        double a = ldg(P + i), b = ldg(P + i + 1);
+        r.p = a + w * (b - a);
+    }
+    if (NEED_TC) {
+        double a = ldg(T + i), b = ldg(T + i + 1);
+        r.T = a + w * (b - a);
+        a = ldg(C + i);
+        b = ldg(C + i + 1);
+        r.cs2 = a + w * (b - a);
+    }
+    return r;
+}
+
+VAH_HD double eos_pressure(const Eos &eos, double e) {
+    if (eos.kind == 0) return e / 3;  // EquationOfState.cpp:78
+    return table_lookup<true, false>(eos.tab, e).p;
+}
+
+// (T, c_s^2); the conformal c_s^2 is the reference's integer `1/3` = 0
+// (EquationOfState.cpp:113).
+VAH_HD void eos_T_cs2(const Eos &eos, double e, double *T, double *cs2) {
+    if (eos.kind == 0) {
+        *T = conformal_T(eos, e);
+        *cs2 = 0.0;
+        return;
+    }
+    EosPoint r = table_lookup<false, true>(eos.tab, e);
+    *T = r.T;
+    *cs2 = r.cs2;
+}
+
+// zeta/s(T), T in fm^-1: the reference's parameterisation (SourceTerms.cpp:
+// 22-44) or the crossover one (height 0.05 at 155 MeV, half-width 50 MeV).
+VAH_HD double zeta_over_s(const Eos &eos, double T) {
+    if (eos.zeta == 1) {
+        const double tp = 0.155 / kHbarc, w = 0.050 / kHbarc;
+        double d = (T - tp) / w;
+        return 0.05 / (1.0 + d * d);
+    }
+    double x = T / 1.01355;
+    if (x > 1.05) return 0.9 * exp(-(x - 1) / 0.025) + 0.25 * exp(-(x - 1) / 0.13) + 0.001;
+    if (x < 0.995) return 0.9 * exp((x - 1) / 0.0025) + 0.22 * exp((x - 1) / 0.022) + 0.03;
+    return -13.77 * x * x + 27.55 * x - 13.45;
+}
+
+// --------------------------------------------------------------- limiter --
+// minmod(x, y) = (sign x + sign y) min(|x|,|y|) / 2 with sign(0) = +1
+// (FluxLimiter.cpp:15-22): equal to +-min(|x|,|y|) when the signs agree, else 0.
+VAH_HD double minmod2(double x, double y) {
+    bool nx = x < 0.0, ny = y < 0.0;
+    double m = fmin(fabs(x), fabs(y));
+    return nx == ny ? (nx ? -m : m) : 0.0;
+}
+
+// FluxLimiter.cpp:28-33, theta = 1.1.
+VAH_HD double approx_derivative(double x, double y, double z) {
+    double l = 1.1 * (y - x);
+    double c = (z - x) * 0.5;
+    double r = 1.1 * (z - y);
+    return minmod2(l, minmod2(c, r));
+}
+
+// ------------------------------------------------------------- inversion --
+// Conserved (T^{tau mu}, P_L, pi^{tau mu}, Pi) -> (e, p, u^mu) by Newton on
+// u_T (EnergyMomentumTensor.cpp:30-197): relative tolerance 1e-7, at most
+// 10^4 iterations; on failure e = 0.999 ePrev, u = (1,0,0,0).
+// Returns 0 (converged), 1 (fallback) or 2 (a NaN reached e or u).
+// out = {e, p, ut, ux, uy, un}.
+template <int PHYS>
+VAH_HD int invert(const Eos &eos, double t, const double *q, double ePrev, double uT0, double *out) {
+    double pitt = 0, pitx = 0, pity = 0, pitn = 0, bulk = 0;
+    if (Phys<PHYS>::PIMUNU) {
+        pitt = q[5];
+        pitx = q[6];
+        pity = q[7];
+        pitn = q[8];
+    }
+    if (Phys<PHYS>::BULK) bulk = q[kSlotPi];
+    const double pl = q[kSlotPL];
+    const double m0 = q[0] - pitt, m1 = q[1] - pitx, m2 = q[2] - pity, m3 = q[3] - pitn;
+    double m0pl = m0 + pl;
+    if (m0pl == 0.0) m0pl = 1.e-16;
+    const double F = m3 / m0pl;  // W off: F = A
+    const double Ft = t * F;
+    const double Ft2 = Ft * Ft;
+    const double x = sqrt(fabs(1. - Ft2));
+    double mbt = sqrt(m1 * m1 + m2 * m2);
+    if (mbt == 0.0) mbt = 1.e-16;
+
+    const double bT = x * mbt;
+    const double bL = x * x * m0 - Ft2 * pl;
+    const double b = x * x + Ft2;
+    const double c0 = m0 - t * Ft * m3;
+    double w = uT0, uT = uT0;
+    int status = 1;
+    for (int it = 0; it < 10000; ++it) {
+        const double w2 = 1 + w * w;
+        const double r = rsqrt_d(w2);
+        const double v = w * r;
+        const double e = c0 - v * x * mbt;
+        if (e < 0.0) break;
+        const double g = bL + b * (0.5 * (e - pl) + 1.5 * bulk);
+        const double r3 = r * r * r;
+        const double f = v * g - bT;
+        double fp = r3 * g + v * b * (0.5 * (-bT * r3));
+        if (fabs(fp) == 0.0) fp = 1.e-16;
+        const double next = w - f / fp;
+        uT = next;
+        if (isnan(next) || isinf(next) || next < 0 || next > 9.0072e+15) break;
+        if (fabs(next - w) <= 1.e-7 * fabs(next)) {
+            status = 0;
+            break;
+        }
+        w = next;
+    }
+    double e, ut, ux, uy, un;
+    if (status == 0) {
+        const double C = sqrt(1.0 + uT * uT);
+        const double U = uT / C;
+        const double inv_mbt = 1.0 / mbt, inv_x = 1.0 / x;
+        ux = uT * m1 * inv_mbt;
+        uy = uT * m2 * inv_mbt;
+        un = F * C * inv_x;
+        ut = C * inv_x;
+        e = c0 - U * x * mbt;
+    } else {
+        e = ePrev * .999;
+        ux = 0.0;
+        uy = 0.0;
+        un = 0.0;
+        ut = 1.0;
+    }
+    out[0] = e;
+    out[1] = eos_pressure(eos, e);
+    out[2] = ut;
+    out[3] = ux;
+    out[4] = uy;
+    out[5] = un;
+    if (isnan(e) || isnan(ut) || isnan(ux) || isnan(uy) || isnan(un)) return 2;
+    return status;
+}
+
+// ------------------------------------------------------------ face flux --
+// Kurganov-Tadmor central flux at one face from the reconstructed states
+// (SemiDiscreteKurganovTadmorScheme.cpp:13-57, SpectralRadius.cpp:14-24,
+// LocalPropagationSpeed.cpp:14-22, FluxFunctions.cpp:15-25):
+// H = (F(qR) + F(qL) - a (qR - qL)) / 2, F = v_dir q, a = max |v_dir|.
+// Returns the number of the two inversions that fell back; bit 8 flags a NaN.
+template <int PHYS>
+VAH_HD int face_flux(const Eos &eos, double t, const double *qR, const double *qL, int dir, double ePrev,
+                     double uT, double *H) {
+    constexpr int NQ = Phys<PHYS>::NQ;
+    double R[6], L[6];
+    const int sR = invert<PHYS>(eos, t, qR, ePrev, uT, R);
+    const int sL = invert<PHYS>(eos, t, qL, ePrev, uT, L);
+    const double vR = R[3 + dir] / R[2], vL = L[3 + dir] / L[2];
+    const double a = fmax(fabs(vL), fabs(vR));
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) H[n] = 0.5 * (vR * qR[n] + vL * qL[n] - a * (qR[n] - qL[n]));
+    return (sR != 0) + (sL != 0) + ((sR == 2 || sL == 2) ? 256 : 0);
+}
+
+// ------------------------------------------------------- axis sources --
+// pi/Pi gradient terms of the T^{tau mu} equations along one axis
+// (SourceTerms.cpp:46-176). d[n] = (q[+1] - q[-1]) / (2h) for the pi fields.
+template <int PHYS>
+VAH_HD void axis_sources(const double *d, int dir, double ucomp, double ut, double t, double *S) {
+    const double v = ucomp / ut;
+    const double dPi = Phys<PHYS>::BULK ? d[kSlotPi] * 1.5 : 0.0;
+    if (dir == 0) {
+        S[0] = d[5] * v - d[6] - v * dPi;
+        S[1] = d[6] * v - d[9] - dPi;
+        S[2] = d[7] * v - d[10];
+        S[3] = d[8] * v - d[11];
+    } else if (dir == 1) {
+        S[0] = d[5] * v - d[7] - v * dPi;
+        S[2] = d[7] * v - d[12] - dPi;
+        S[1] = d[6] * v - d[10];
+        S[3] = d[8] * v - d[13];
+    } else {
+        const float tf = (float)t;  // SourceTerms.cpp:172: powf(t, 2)
+        S[0] = d[5] * v - d[8] - v * dPi;
+        S[3] = d[8] * v - d[14] - dPi / (double)(tf * tf);
+        S[1] = d[6] * v - d[11];
+        S[2] = d[7] * v - d[13];
+    }
+}
+
+// ----------------------------------------------------------- cell sources --
+// Inputs of the local source terms at one cell: stage-input conserved values,
+// primitives, previous-stage velocity and central differences (q(+1)-q(-1))/(2h).
+struct CellGrad {
+    double e, p, ut, ux, uy, un;
+    double utp, uxp, uyp, unp;
+    double dxut, dxux, dxuy, dxun, dyut, dyux, dyuy, dyun, dnut, dnux, dnuy, dnun;
+    double dxp, dyp, dnp, dxe, dye, dne, dxpl, dypl, dnpl;
+};
+
+// Geometric and relaxation sources S[n] (SourceTerms.cpp:178-1044), W off.
+template <int PHYS>
+VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, double t, double dt, double etabar,
+                        double *S) {
+    constexpr bool PIM = Phys<PHYS>::PIMUNU, BULK = Phys<PHYS>::BULK;
+    const double ttt = Q[0], ttx = Q[1], tty = Q[2], ttn = Q[3], pl = Q[4];
+    double pitt = 0, pitx = 0, pity = 0, pitn = 0, pixx = 0, pixy = 0, pixn = 0, piyy = 0, piyn = 0, pinn = 0,
+           Pi = 0;
+    if (PIM) {
+        pitt = Q[5]; pitx = Q[6]; pity = Q[7]; pitn = Q[8]; pixx = Q[9];
+        pixy = Q[10]; pixn = Q[11]; piyy = Q[12]; piyn = Q[13]; pinn = Q[14];
+    }
+    if (BULK) Pi = Q[kSlotPi];
+    double e = g.e;
+    const double p = g.p, ut = g.ut, ux = g.ux, uy = g.uy, un = g.un;
+    const double dxut = g.dxut, dxux = g.dxux, dxuy = g.dxuy, dxun = g.dxun;
+    const double dyut = g.dyut, dyux = g.dyux, dyuy = g.dyuy, dyun = g.dyun;
+    const double dnut = g.dnut, dnux = g.dnux, dnuy = g.dnuy, dnun = g.dnun;
+
+    const double inv_ut = 1.0 / ut, inv_t = 1.0 / t;
+    const double vx = ux * inv_ut, vy = uy * inv_ut, vn = un * inv_ut;
+    const double dkvk = (dxux - vx * dxut) * inv_ut + (dyuy - vy * dyut) * inv_ut + (dnun - vn * dnut) * inv_ut;
+
+    const double t2 = t * t, t3 = t * t2, un2 = un * un, ut2 = ut * ut;
+    const double inv_t2 = 1.0 / t2;
+
+    // velocity gradients (SourceTerms.cpp:301-334)
+    const double inv_dt = 1.0 / dt;
+    const double dtut = (ut - g.utp) * inv_dt, dtux = (ux - g.uxp) * inv_dt;
+    const double dtuy = (uy - g.uyp) * inv_dt, dtun = (un - g.unp) * inv_dt;
+    const double dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;
+    const double duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
+    const double dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
+    const double dut = ut * dtut + ux * dxut + uy * dyut + un * dnut;  // = Dut - t un^2
+    const double Dut = dut + t * un2;
+    const double Dux = -dux, Duy = -duy;
+    const double Dun = -t2 * (dun + 2 * ut * un * inv_t);
+    const double theta = ut * inv_t + dtut + dxux + dyuy + dnun;
+    const double th3 = theta / 3;
+
+    const double stt = -t * ut * un2 + (dtut - ut * dut) + (ut2 - 1) * th3;
+    const double stx = -(t * un2 * ux) * 0.5 + (dtux - dxut) * 0.5 - (ux * dut + ut * dux) * 0.5 + ut * ux * th3;
+    const double sty = -(t * un2 * uy) * 0.5 + (dtuy - dyut) * 0.5 - (uy * dut + ut * duy) * 0.5 + ut * uy * th3;
+    const double stn = -un * (2 * ut2 + t2 * un2) * (0.5 * inv_t) + (dtun - dnut * inv_t2) * 0.5 -
+                       (un * dut + ut * dun) * 0.5 + ut * un * th3;
+    const double sxx = -(dxux + ux * dux) + (1 + ux * ux) * th3;
+    const double sxy = -(dxuy + dyux) * 0.5 - (uy * dux + ux * duy) * 0.5 + ux * uy * th3;
+    const double sxn = -ut * ux * un * inv_t - (dxun + dnux * inv_t2) * 0.5 - (un * dux + ux * dun) * 0.5 + ux * un * th3;
+    const double syy = -(dyuy + uy * duy) + (1 + uy * uy) * th3;
+    const double syn = -ut * uy * un * inv_t - (dyun + dnuy * inv_t2) * 0.5 - (un * duy + uy * dun) * 0.5 + uy * un * th3;
+    const double snn = -ut * (1 + 2 * t2 * un2) / t3 - dnun * inv_t2 - un * dun + (inv_t2 + un2) * th3;
+
+    // transverse / longitudinal split (SourceTerms.cpp:355-426)
+    const double uT2 = ux * ux + uy * uy;
+    const double uTdxuT = ux * dxux + uy * dxuy;
+    const double uTdyuT = ux * dyux + uy * dyuy;
+    const double uTdnuT = ux * dnux + uy * dnuy;
+    const double uTduT = ut * (ux * dtux + uy * dtuy) + ux * uTdxuT + uy * uTdyuT + un * uTdnuT;
+    const double F = 1 + uT2;
+    const double inv_F = 1.0 / F;
+    const double F2 = F * F;
+    const double inv_sF = rsqrt_d(F);
+    const double z0 = t * un * inv_sF;
+    const double z3 = ut * inv_t * inv_sF;
+    const double z02 = z0 * z0, z0z3 = z0 * z3, z32 = z3 * z3;
+    const double dz0 = (ut * un + t * dun - t * un * inv_F * uTduT) * inv_sF;
+    const double dz3 = (-ut2 * inv_t2 + dut * inv_t - ut * inv_t * inv_F * uTduT) * inv_sF;
+    const double Dz0 = dz0 + t * un * z3;
+    const double Dz3 = -t2 * (dz3 + (ut * z3 + un * z0) * inv_t);
+    const double A = z02 * stt - 2 * t2 * z0z3 * stn + t2 * t2 * z32 * snn;
+    const double B0 = z0 * stt - t2 * z3 * stn;
+    const double B1 = z0 * stx - t2 * z3 * sxn;
+    const double B2 = z0 * sty - t2 * z3 * syn;
+    const double B3 = z0 * stn - t2 * z3 * snn;
+    const double thetaT = 2 * th3 + A;
+    const double zDzu = theta - thetaT;
+    const double sttT = stt + 2 * z0 * B0 + z02 * A - 0.5 * (1 - ut * ut + z02) * A;
+    const double stxT = stx + z0 * B1 - 0.5 * (-ut * ux) * A;
+    const double styT = sty + z0 * B2 - 0.5 * (-ut * uy) * A;
+    const double stnT = stn + z0 * B3 + z3 * B0 + z0z3 * A - 0.5 * (-ut * un + z0z3) * A;
+    const double sxxT = sxx - 0.5 * (-1 - ux * ux) * A;
+    const double sxyT = sxy - 0.5 * (-ux * uy) * A;
+    const double sxnT = sxn + z3 * B1 - 0.5 * (-ux * un) * A;
+    const double syyT = syy - 0.5 * (-1 - uy * uy) * A;
+    const double synT = syn + z3 * B2 - 0.5 * (-uy * un) * A;
+    const double snnT = snn + 2 * z3 * B3 + z32 * A - 0.5 * (-inv_t2 - un * un + z32) * A;
+
+    // closures (SourceTerms.cpp:431-481)
+    if (e == 0) e = 1.e-7;
+    double T, cs2;
+    eos_T_cs2(eos, e, &T, &cs2);
+    const double inv_e = 1.0 / e;
+    double ap[16];
+    ap[0] = 1.0;
+    ap[1] = pl * inv_e;
+#pragma unroll
+    for (int k = 2; k < 16; ++k) ap[k] = ap[k - 1] * ap[1];
+    const double a = ap[1];
+    const double Rtilde = poly::Rtilde(ap);
+    const double Rbar0 = poly::Rbar0(ap);
+    const double Rgamma = poly::Rgamma(ap);
+    const double Rbar0P = poly::Rbar0P(ap);
+
+    const double e3p = e - 3 * p;
+    const double ptHat = (e - pl - Rbar0 * e3p) * 0.5;
+    const double pt = ptHat + 1.5 * Pi;
+    const double DP = pl - pt;
+    const double Ltt = DP * t2 * un2 * inv_F;
+    const double Ltn = DP * ut * un * inv_F;
+    const double Lnn = DP * ut2 * inv_F * inv_t2;
+    const double tnn = (e + pt) * un * un + pt * inv_t2 + Lnn + pinn;
+
+    const double dxRbar0 = Rbar0P * (g.dxpl - a * g.dxe) * inv_e;
+    const double dyRbar0 = Rbar0P * (g.dypl - a * g.dye) * inv_e;
+    const double dnRbar0 = Rbar0P * (g.dnpl - a * g.dne) * inv_e;
+    const double dxptHat = 0.5 * (g.dxe - g.dxpl - Rbar0 * (g.dxe - 3 * g.dxp) - e3p * dxRbar0);
+    const double dyptHat = 0.5 * (g.dye - g.dypl - Rbar0 * (g.dye - 3 * g.dyp) - e3p * dyRbar0);
+    const double dnptHat = 0.5 * (g.dne - g.dnpl - Rbar0 * (g.dne - 3 * g.dnp) - e3p * dnRbar0);
+    const double dxDP = g.dxpl - dxptHat, dyDP = g.dypl - dyptHat, dnDP = g.dnpl - dnptHat;
+
+    const double inv_F2 = inv_F * inv_F;
+    const double dxLtt = (2 * DP * dxun * t2 * un) * inv_F + (dxDP * t2 * un2) * inv_F - (2 * DP * uTdxuT * t2 * un2) * inv_F2;
+    const double dyLtt = (2 * DP * dyun * t2 * un) * inv_F + (dyDP * t2 * un2) * inv_F - (2 * DP * uTdyuT * t2 * un2) * inv_F2;
+    const double dnLtt = (2 * DP * dnun * t2 * un) * inv_F + (dnDP * t2 * un2) * inv_F - (2 * DP * uTdnuT * t2 * un2) * inv_F2;
+    const double dxLtn = (DP * dxut * un) * inv_F + (DP * dxun * ut) * inv_F + (dxDP * un * ut) * inv_F -
+                         (2 * DP * uTdxuT * un * ut) * inv_F2;
+    const double dyLtn = (DP * dyut * un) * inv_F + (DP * dyun * ut) * inv_F + (dyDP * un * ut) * inv_F -
+                         (2 * DP * uTdyuT * un * ut) * inv_F2;
+    const double dnLtn = (DP * dnut * un) * inv_F + (DP * dnun * ut) * inv_F + (dnDP * un * ut) * inv_F -
+                         (2 * DP * uTdnuT * un * ut) * inv_F2;
+    const double dnLnn = ((2 * DP * dnut * ut) * inv_F + (dnDP * ut2) * inv_F - (2 * DP * uTdnuT * ut2) * inv_F2) * inv_t2;
+    (void)F2;
+
+    const double zeta_zz = Rtilde * e - 3 * pl;
+    const double zeta_zT = (Rtilde * e + pl) * 0.5;
+    const double delta_pipi = (3 + Rgamma) * 0.5;
+    const double tau_pipi = 4 * delta_pipi / 3;  // SourceTerms.cpp:634, 1/2 -> 0
+    const double lambda_pipi = Rgamma - 1;
+    const double taupiInv = 0.2 * T / etabar;
+
+    const double psT = pitt * sttT - 2 * pitx * stxT - 2 * pity * styT + pixx * sxxT + 2 * pixy * sxyT + piyy * syyT -
+                       2 * pitn * stnT * t2 + 2 * pixn * sxnT * t2 + 2 * piyn * synT * t2 + pinn * snnT * t2 * t2;
+
+    double beta_lPi = 0, delta_lPi = 0, beta_PiPi = 0, delta_PiPi = 0, lambda_Pipi = 0;
+    if (BULK) {
+        // AnisotropicDistributionFunctions.cpp:73-190 (2/9 -> 0, 3/2 -> 1, 1/3 -> 0)
+        double third = 1.0 / 3.0 - cs2;
+        if (third == 0.0) third = 1.e-16;
+        const double meq2 = 36 * third;
+        const double z2logz = -2 * (1 + 0.02536 * meq2);
+        const double g40 = (poly::g0m2040DividedBym2LogZTerm(ap) * z2logz + poly::g0m2040DividedBym2Zm2Term(ap)) / meq2 +
+                           poly::g0m2040DividedBym2ConstantTerm(ap);
+        const double g20c = poly::g0m2020ConstantTerm(ap);
+        const double g20 = g20c + poly::g0m2020Z2LogZTerm(ap) * z2logz + poly::g0m2020Z2Term(ap) * meq2;
+        beta_lPi = 3 * g40;
+        delta_lPi = g20 + g40;
+        beta_PiPi = 1 - g20c;
+        delta_PiPi = 0.5 * (1 + g20c);
+        lambda_Pipi = 3 * poly::G_G1(ap) / 5 * (0 - cs2);
+    }
+
+    const double dPL = -(pl - p) * taupiInv + zeta_zz * zDzu - zeta_zT * thetaT - beta_lPi * Pi * zDzu -
+                       delta_lPi * Pi * thetaT - Rgamma * psT;
+    S[4] = dPL * inv_ut + dkvk * pl;
+
+    S[0] = -(ttt * inv_t + t * tnn) + dkvk * (Ltt + pitt - pt) - vx * dxptHat - vy * dyptHat - vn * dnptHat +
+           vx * dxLtt + vy * dyLtt + vn * dnLtt - dnLtn;
+    S[1] = -ttx * inv_t - dxptHat + dkvk * pitx;
+    S[2] = -tty * inv_t - dyptHat + dkvk * pity;
+    // SourceTerms.cpp:686: the reference adds dnLtn twice
+    S[3] = -3 * ttn * inv_t - dnptHat * inv_t2 + dkvk * (Ltn + pitn) + vx * dxLtn + vy * dyLtn + vn * (dnLtn + dnLtn) - dnLnn;
+    int bad = isnan(S[4]) || isnan(S[0]);
+
+    if (PIM) {
+        // SourceTerms.cpp:725-930; the I6/I7 and lambda_piPi terms vanish with W off
+        const double etaBar_TC = ((3 - Rtilde) * e - 2 * pl) * 0.125;
+        const double I1tt = 2 * ut * (pitt * Dut + pitx * Dux + pity * Duy + pitn * Dun) - 2 * z0 * (pitt * Dz0 + pitn * Dz3);
+        const double I1tx = (pitt * ux + pitx * ut) * Dut + (pitx * ux + pixx * ut) * Dux + (pity * ux + pixy * ut) * Duy +
+                            (pitn * ux + pixn * ut) * Dun - ((pitx * z0) * Dz0 + (pitn * ux + pixn * z0) * Dz3);
+        const double I1ty = (pitt * uy + pity * ut) * Dut + (pitx * uy + pixy * ut) * Dux + (pity * uy + piyy * ut) * Duy +
+                            (pitn * uy + piyn * ut) * Dun - ((pity * z0) * Dz0 + (pitn * uy + piyn * z0) * Dz3);
+        const double I1tn = (pitt * un + pitn * ut) * Dut + (pitx * un + pixn * ut) * Dux + (pity * un + piyn * ut) * Duy +
+                            (pitn * un + pinn * ut) * Dun - ((pitt * z3 + pitn * z0) * Dz0 + (pitn * z3 + pinn * z0) * Dz3);
+        const double I1xx = 2 * ux * (pitx * Dut + pixx * Dux + pixy * Duy + pixn * Dun);
+        const double I1xy = (pitx * uy + pity * ux) * Dut + (pixx * uy + pixy * ux) * Dux + (pixy * uy + piyy * ux) * Duy +
+                            (pixn * uy + piyn * ux) * Dun;
+        const double I1xn = (pitx * un + pitn * ux) * Dut + (pixx * un + pixn * ux) * Dux + (pixy * un + piyn * ux) * Duy +
+                            (pixn * un + pinn * ux) * Dun - ((pitx * z3) * Dz0 + (pixn * z3) * Dz3);
+        const double I1yy = 2 * uy * (pity * Dut + pixy * Dux + piyy * Duy + piyn * Dun);
+        const double I1yn = (pity * un + pitn * uy) * Dut + (pixy * un + pixn * uy) * Dux + (piyy * un + piyn * uy) * Duy +
+                            (piyn * un + pinn * uy) * Dun - ((pity * z3) * Dz0 + (piyn * z3) * Dz3);
+        const double I1nn = 2 * un * (pitn * Dut + pixn * Dux + piyn * Duy + pinn * Dun) - 2 * z3 * (pitn * Dz0 + pinn * Dz3);
+
+        const double ps2 = psT * 0.5;
+        const double I4tt = (pitt * sttT - pitx * stxT - pity * styT - t2 * pitn * stnT) - (1 - ut2 + z02) * ps2;
+        const double I4tx = (pitt * stxT + pitx * sttT) * 0.5 - (pitx * sxxT + pixx * stxT) * 0.5 -
+                            (pity * sxyT + pixy * styT) * 0.5 - t2 * (pitn * sxnT + pixn * stnT) * 0.5 + (ut * ux) * ps2;
+        const double I4ty = (pitt * styT + pity * sttT) * 0.5 - (pitx * sxyT + pixy * stxT) * 0.5 -
+                            (pity * syyT + piyy * styT) * 0.5 - t2 * (pitn * synT + piyn * stnT) * 0.5 + (ut * uy) * ps2;
+        const double I4tn = (pitt * stnT + pitn * sttT) * 0.5 - (pitx * sxnT + pixn * stxT) * 0.5 -
+                            (pity * synT + piyn * styT) * 0.5 - t2 * (pitn * snnT + pinn * stnT) * 0.5 +
+                            (ut * un - z0z3) * ps2;
+        const double I4xx = (pitx * stxT - pixx * sxxT - pixy * sxyT - t2 * pixn * sxnT) + (1 + ux * ux) * ps2;
+        const double I4xy = (pitx * styT + pity * stxT) * 0.5 - (pixx * sxyT + pixy * sxxT) * 0.5 -
+                            (pixy * syyT + piyy * sxyT) * 0.5 - t2 * (pixn * synT + piyn * sxnT) * 0.5 + (ux * uy) * ps2;
+        const double I4xn = (pitx * stnT + pitn * stxT) * 0.5 - (pixx * sxnT + pixn * sxxT) * 0.5 -
+                            (pixy * synT + piyn * sxyT) * 0.5 - t2 * (pixn * snnT + pinn * sxnT) * 0.5 + (ux * un) * ps2;
+        const double I4yy = (pity * styT - pixy * sxyT - piyy * syyT - t2 * piyn * synT) + (1 + uy * uy) * ps2;
+        const double I4yn = (pity * stnT + pitn * styT) * 0.5 - (pixy * sxnT + pixn * sxyT) * 0.5 -
+                            (piyy * synT + piyn * syyT) * 0.5 - t2 * (piyn * snnT + pinn * synT) * 0.5 + (uy * un) * ps2;
+        const double I4nn = (pitn * stnT - pixn * sxnT - piyn * synT - t2 * pinn * snnT) + (inv_t2 + un2 - z32) * ps2;
+
+        const double c2 = delta_pipi * thetaT + lambda_pipi * zDzu;  // I2, I5 both scale pi
+        const double two_eta = 2 * etaBar_TC;
+        const double dpitt = two_eta * sttT - pitt * taupiInv - (I1tt - c2 * pitt + tau_pipi * I4tt) - 2 * un * t * pitn;
+        const double dpitx = two_eta * stxT - pitx * taupiInv - (I1tx - c2 * pitx + tau_pipi * I4tx) - un * t * pixn;
+        const double dpity = two_eta * styT - pity * taupiInv - (I1ty - c2 * pity + tau_pipi * I4ty) - un * t * piyn;
+        const double dpitn = two_eta * stnT - pitn * taupiInv - (I1tn - c2 * pitn + tau_pipi * I4tn) - un * t * pinn -
+                             (ut * pitn + un * pitt) * inv_t;
+        const double dpixx = two_eta * sxxT - pixx * taupiInv - (I1xx - c2 * pixx + tau_pipi * I4xx);
+        const double dpixy = two_eta * sxyT - pixy * taupiInv - (I1xy - c2 * pixy + tau_pipi * I4xy);
+        const double dpixn = two_eta * sxnT - pixn * taupiInv - (I1xn - c2 * pixn + tau_pipi * I4xn) - (ut * pixn + un * pitx) * inv_t;
+        const double dpiyy = two_eta * syyT - piyy * taupiInv - (I1yy - c2 * piyy + tau_pipi * I4yy);
+        const double dpiyn = two_eta * synT - piyn * taupiInv - (I1yn - c2 * piyn + tau_pipi * I4yn) - (ut * piyn + un * pity) * inv_t;
+        const double dpinn = two_eta * snnT - pinn * taupiInv - (I1nn - c2 * pinn + tau_pipi * I4nn) - 2 * (ut * pinn + un * pitn) * inv_t;
+        S[5] = dpitt * inv_ut + pitt * dkvk;
+        S[6] = dpitx * inv_ut + pitx * dkvk;
+        S[7] = dpity * inv_ut + pity * dkvk;
+        S[8] = dpitn * inv_ut + pitn * dkvk;
+        S[9] = dpixx * inv_ut + pixx * dkvk;
+        S[10] = dpixy * inv_ut + pixy * dkvk;
+        S[11] = dpixn * inv_ut + pixn * dkvk;
+        S[12] = dpiyy * inv_ut + piyy * dkvk;
+        S[13] = dpiyn * inv_ut + piyn * dkvk;
+        S[14] = dpinn * inv_ut + pinn * dkvk;
+    }
+    if (BULK) {
+        // SourceTerms.cpp:1030-1042
+        const double Rhat = poly::Rhat(ap);
+        const double bb = 1.0 / 3.0 - cs2;
+        const double tauPiInv = 15 * bb * bb * T / zeta_over_s(eos, T);
+        const double zeta_z = (Rhat - Rbar0) * e3p / 3;
+        const double zeta_T = -(Rbar0 + Rhat) * e3p / 6;
+        const double dPi = -((1 - Rbar0) * e3p / 3 + Pi) * tauPiInv - zeta_z * zDzu - zeta_T * thetaT -
+                           beta_PiPi * Pi * zDzu - delta_PiPi * Pi * thetaT + lambda_Pipi * psT;
+        S[kSlotPi] = dPi * inv_ut + Pi * dkvk;
+    }
+    return bad;
+}
+
+// -------------------------------------------------------------- regulator --
+// FullyDiscreteKurganovTadmorScheme.cpp:524-696: e < 0 -> e = p = 1e-7,
+// P_L < 0 -> 1e-7, then pi^{mu nu} *= tanh(rho)/rho (xi0 = rho_max = 1).
+template <int PHYS>
+VAH_HD void regulate(double t, double &e, double &p, double *q, const double *u) {
+    if (e < 0.0) {
+        e = 1.e-7;
+        p = 1.e-7;
+    }
+    if (q[kSlotPL] < 0.0) q[kSlotPL] = 1.e-7;
+    if (!Phys<PHYS>::PIMUNU) return;
+    const double pl = q[kSlotPL];
+    double ap[9];
+    ap[0] = 1.0;
+    ap[1] = pl / e;
+#pragma unroll
+    for (int k = 2; k < 9; ++k) ap[k] = ap[k - 1] * ap[1];
+    const double ptHat = (e - pl - poly::Rbar0(ap) * (e - 3 * p)) * 0.5;
+    const double pitt = q[5], pitx = q[6], pity = q[7], pitn = q[8], pixx = q[9];
+    const double pixy = q[10], pixn = q[11], piyy = q[12], piyn = q[13], pinn = q[14];
+    const double ut = u[0], ux = u[1], uy = u[2], un = u[3];
+    const double inv_sF = rsqrt_d(1 + (ux * ux + uy * uy));
+    const double z0 = t * un * inv_sF;
+    const double z3 = ut / t * inv_sF;
+    const double t2 = t * t;
+    const double sTrsTrs = sqrt(fabs(e * e + pl * pl + 2 * ptHat * ptHat));
+    const double pipi = pitt * pitt - 2 * pitx * pitx - 2 * pity * pity + pixx * pixx + 2 * pixy * pixy + piyy * piyy -
+                        2 * pitn * pitn * t2 + 2 * pixn * pixn * t2 + 2 * piyn * piyn * t2 + pinn * pinn * t2 * t2;
+    const double spipi = sqrt(fabs(pipi));
+    double rho = spipi / sTrsTrs;
+    const double den = spipi;
+    const double cand[9] = {(pitt - pixx - piyy - pinn * t2) / den,
+                            (-pitn * t2 * un + pitt * ut - pitx * ux - pity * uy) / den,
+                            (-pixn * t2 * un + pitx * ut - pixx * ux - pixy * uy) / den,
+                            (-piyn * t2 * un + pity * ut - pixy * ux - piyy * uy) / den,
+                            (-pinn * t2 * un + pitn * ut - pixn * ux - piyn * uy) / den,
+                            (z0 * pitt - t2 * z3 * pitn) / den,
+                            (z0 * pitx - t2 * z3 * pixn) / den,
+                            (z0 * pity - t2 * z3 * piyn) / den,
+                            (z0 * pitn - t2 * z3 * pinn) / den};
+#pragma unroll
+    for (int m = 0; m < 9; ++m)
+        if (cand[m] > rho) rho = cand[m];
+    double fac = tanh(rho) / rho;
+    if (rho < 1.e-7) fac = 1.0;
+#pragma unroll
+    for (int n = 5; n < 15; ++n) q[n] *= fac;
+}
+
+}  // namespace vah

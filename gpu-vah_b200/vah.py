@@ -1,0 +1,220 @@
+"""Python binding of libvah.so (include/vah.h) through ctypes.
+
+The library is the product; this module only loads it and wraps the C ABI
+for Python callers (tests, bench, notebooks). There is no Python or CPU
+implementation of the step behind it: if libvah.so is missing or no CUDA
+device is present, creating an event raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+D, I, P = C.c_double, C.c_int, C.POINTER(C.c_double)
+
+# include/vah.h constants
+VAH_IDEAL, VAH_PIMUNU, VAH_PIMUNU_PI = 0, 1, 2
+VAH_EOS_CONFORMAL, VAH_EOS_TABLE = 0, 1
+VAH_ZETA_REFERENCE, VAH_ZETA_CROSSOVER = 0, 1
+VAH_FP64, VAH_FP32 = 0, 1
+VAH_FLUX_PER_CELL, VAH_FLUX_SHARED = 0, 1
+VAH_PL_REFERENCE, VAH_PL_ISOTROPIC = 0, 1
+NUM_FIELDS = 26
+F_E, F_P, F_UT, F_UX, F_UY, F_UN = 16, 17, 18, 19, 20, 21
+HBARC = 0.197326938
+
+STATUS = {0: "VAH_OK", -1: "VAH_ERR_ARG", -2: "VAH_ERR_CUDA", -3: "VAH_ERR_NOMEM", -4: "VAH_ERR_NAN",
+          -5: "VAH_ERR_NODEVICE", -6: "VAH_ERR_TOO_LARGE"}
+
+
+class VahError(RuntimeError):
+    def __init__(self, where, rc):
+        super().__init__(f"{where} failed: {STATUS.get(rc, rc)}")
+        self.rc = rc
+
+
+def check(rc, where):
+    if rc != 0:
+        raise VahError(where, rc)
+
+
+class Lattice(C.Structure):
+    _fields_ = [("nx", I), ("ny", I), ("nz", I), ("dx", D), ("dy", D), ("dz", D)]
+
+
+class Hydro(C.Structure):
+    _fields_ = [("t0", D), ("eta_over_s", D), ("freezeout_T_GeV", D)]
+
+
+class Options(C.Structure):
+    _fields_ = [("physics", I), ("eos", I), ("zeta", I), ("precision", I), ("flux", I), ("device", I),
+                ("stream", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("face_fallbacks", C.c_longlong), ("cell_fallbacks", C.c_longlong), ("nan_cells", C.c_longlong),
+                ("steps", C.c_longlong)]
+
+
+EXPORTS = ["vah_version", "vah_eos_table_build", "vah_event_create", "vah_event_destroy", "vah_event_set_field",
+           "vah_event_get_field", "vah_event_set_conserved", "vah_event_init_from_e", "vah_event_set_ghost_cells",
+           "vah_rk2_step", "vah_run", "vah_event_sync", "vah_event_stats", "vah_event_set_timing",
+           "vah_event_kernel_time", "vah_rk2_step_host", "vah_ic_optical_glauber", "vah_ic_mc_glauber",
+           "vah_ic_longitudinal"]
+
+_lib = None
+
+
+def lib_path():
+    return os.path.join(HERE, "libvah.so")
+
+
+def library():
+    """Load libvah.so (built in-tree by __graft_entry__.build())."""
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise RuntimeError(f"libvah.so is not built ({path})")
+        L = C.CDLL(path)
+        L.vah_version.restype = C.c_char_p
+        L.vah_eos_table_build.argtypes = [I, P, C.c_size_t]
+        L.vah_event_create.argtypes = [C.POINTER(Lattice), C.POINTER(Hydro), C.POINTER(Options), P,
+                                       C.POINTER(C.c_void_p)]
+        for name in ("vah_event_destroy", "vah_event_set_ghost_cells", "vah_event_sync"):
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.vah_event_set_field.argtypes = [C.c_void_p, I, P, I]
+        L.vah_event_get_field.argtypes = [C.c_void_p, I, P, I]
+        L.vah_event_set_conserved.argtypes = [C.c_void_p, D, I]
+        L.vah_event_init_from_e.argtypes = [C.c_void_p, D, P, I]
+        L.vah_rk2_step.argtypes = [C.c_void_p, D, D]
+        L.vah_run.argtypes = [C.c_void_p, D, D, I]
+        L.vah_event_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        L.vah_event_set_timing.argtypes = [C.c_void_p, I]
+        L.vah_event_kernel_time.argtypes = [C.c_void_p, P, C.POINTER(C.c_longlong)]
+        L.vah_rk2_step_host.argtypes = [C.c_void_p, D, D, C.POINTER(P)]
+        L.vah_ic_optical_glauber.argtypes = [I, I, D, D, D, D, I, D, D, D, D, D, P]
+        L.vah_ic_mc_glauber.argtypes = [I, I, D, D, D, D, I, D, D, D, C.c_ulonglong, D, D, P, C.POINTER(I)]
+        L.vah_ic_longitudinal.argtypes = [I, D, D, D, P]
+        _lib = L
+    return _lib
+
+
+def version():
+    return library().vah_version().decode()
+
+
+def eos_table(n=4096):
+    """The tabulated crossover EoS (vah_eos_table_build)."""
+    out = np.zeros(8 + 3 * n)
+    check(library().vah_eos_table_build(n, out.ctypes.data_as(P), out.size), "vah_eos_table_build")
+    return out
+
+
+def table_energy_density(tab, T_fm):
+    """e(T) by inverting the table's T(e) (bisection in ln e, host side)."""
+    n = int(tab[0])
+    lne0, dl = tab[1], tab[3]
+    Ts = tab[8 + n:8 + 2 * n]
+    lne = lne0 + dl * np.arange(n)
+    return float(np.exp(np.interp(np.log(T_fm), np.log(Ts), lne)))
+
+
+def optical_glauber(nx, ny, dx, dy, b=7.0, sigma_nn_fm2=4.2, A=197, R=6.38, a=0.535, x_coll=0.15, e_peak=1.0,
+                    e_floor=1e-3):
+    out = np.zeros(nx * ny)
+    check(library().vah_ic_optical_glauber(nx, ny, dx, dy, b, sigma_nn_fm2, A, R, a, x_coll, e_peak, e_floor,
+                                           out.ctypes.data_as(P)), "vah_ic_optical_glauber")
+    return out
+
+
+def mc_glauber(nx, ny, dx, dy, b, seed, sigma_nn_fm2=4.2, A=197, R=6.38, a=0.535, width=0.5, e_peak=1.0,
+               e_floor=1e-3):
+    out = np.zeros(nx * ny)
+    npart = C.c_int()
+    check(library().vah_ic_mc_glauber(nx, ny, dx, dy, b, sigma_nn_fm2, A, R, a, width, seed, e_peak, e_floor,
+                                      out.ctypes.data_as(P), C.byref(npart)), "vah_ic_mc_glauber")
+    return out, npart.value
+
+
+def longitudinal(nz, dz, eta_flat=1.5, sigma_eta=1.3):
+    out = np.zeros(nz)
+    check(library().vah_ic_longitudinal(nz, dz, eta_flat, sigma_eta, out.ctypes.data_as(P)), "vah_ic_longitudinal")
+    return out
+
+
+class Event:
+    """One hydro event on the GPU, through the C ABI."""
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, eta_over_s, physics=VAH_PIMUNU_PI, eos=VAH_EOS_TABLE,
+                 zeta=VAH_ZETA_CROSSOVER, table=None, t0=0.5, precision=VAH_FP64, flux=VAH_FLUX_PER_CELL, device=0,
+                 stream=None):
+        self.L = library()
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.ncell = (nx + 4) * (ny + 4) * (nz + 4)
+        self._table = None if table is None else np.ascontiguousarray(table, dtype=np.float64)
+        lat = Lattice(nx, ny, nz, dx, dy, dz)
+        hyd = Hydro(t0, eta_over_s, 0.155)
+        opt = Options(physics, eos, zeta, precision, flux, device, stream)
+        self.ev = C.c_void_p()
+        tab = self._table.ctypes.data_as(P) if self._table is not None else None
+        check(self.L.vah_event_create(C.byref(lat), C.byref(hyd), C.byref(opt), tab, C.byref(self.ev)),
+              "vah_event_create")
+
+    def close(self):
+        if self.ev:
+            self.L.vah_event_destroy(self.ev)
+            self.ev = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_field(self, fid, arr, with_ghosts=True):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        check(self.L.vah_event_set_field(self.ev, fid, a.ctypes.data_as(P), int(with_ghosts)), "vah_event_set_field")
+
+    def get_field(self, fid, with_ghosts=True):
+        out = np.empty(self.ncell if with_ghosts else self.nx * self.ny * self.nz)
+        check(self.L.vah_event_get_field(self.ev, fid, out.ctypes.data_as(P), int(with_ghosts)), "vah_event_get_field")
+        return out
+
+    def set_conserved(self, t, pl_from_field):
+        check(self.L.vah_event_set_conserved(self.ev, t, int(pl_from_field)), "vah_event_set_conserved")
+
+    def init_from_e(self, t0, e_interior, pl_mode=VAH_PL_ISOTROPIC):
+        a = np.ascontiguousarray(e_interior, dtype=np.float64)
+        check(self.L.vah_event_init_from_e(self.ev, t0, a.ctypes.data_as(P), pl_mode), "vah_event_init_from_e")
+
+    def set_ghost_cells(self):
+        check(self.L.vah_event_set_ghost_cells(self.ev), "vah_event_set_ghost_cells")
+
+    def step(self, t, dt):
+        check(self.L.vah_rk2_step(self.ev, t, dt), "vah_rk2_step")
+
+    def run(self, t0, dt, n):
+        check(self.L.vah_run(self.ev, t0, dt, n), "vah_run")
+
+    def sync(self):
+        check(self.L.vah_event_sync(self.ev), "vah_event_sync")
+
+    def stats(self):
+        s = Stats()
+        check(self.L.vah_event_stats(self.ev, C.byref(s)), "vah_event_stats")
+        return s
+
+    def set_timing(self, on):
+        check(self.L.vah_event_set_timing(self.ev, int(on)), "vah_event_set_timing")
+
+    def kernel_time(self):
+        ms, n = D(), C.c_longlong()
+        check(self.L.vah_event_kernel_time(self.ev, C.byref(ms), C.byref(n)), "vah_event_kernel_time")
+        return ms.value, n.value
+
+    def step_host(self, t, dt, ptrs):
+        """Host-buffer step: ptrs = list of NUM_FIELDS host addresses (0 for unused)."""
+        arr = (P * NUM_FIELDS)(*[C.cast(C.c_void_p(p), P) if p else P() for p in ptrs])
+        check(self.L.vah_rk2_step_host(self.ev, t, dt, arr), "vah_rk2_step_host")

@@ -1,0 +1,213 @@
+/*
+ * vah.h -- C ABI of the B200 VAH time step (libvah.so).
+ *
+ * Drop-in boundary for the anisotropic viscous hydrodynamics step of
+ * derekeverett/GPU-VAH. Plain pointers and sizes only; every call returns an
+ * int status (VAH_OK = 0, < 0 on error) and never exits or traps. Each entry
+ * point names the reference interface it replaces (file:line within the
+ * reference project).
+ *
+ * Data layout (part of the drop-in surface): one array per field, cell
+ * (i, j, k) of an nx*ny*nz interior grid with 2 ghost layers per side at
+ * i + ncx*(j + ncy*k), nc = n + 4, x fastest
+ * (rhic/src/DynamicalVariables.cpp:29-31, rhic/include/LatticeParameters.h:13-15).
+ *
+ * Threading: calls on one event are not thread-safe; distinct events may be
+ * driven from distinct host threads. Work is queued on the event's stream.
+ */
+#ifndef VAH_H
+#define VAH_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define VAH_OK 0
+#define VAH_ERR_ARG (-1)        /* invalid argument */
+#define VAH_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define VAH_ERR_NOMEM (-3)      /* device allocation failed */
+#define VAH_ERR_NAN (-4)        /* a NaN reached e or u (reference: exit(-1)) */
+#define VAH_ERR_NODEVICE (-5)   /* no CUDA device / kernels not loadable */
+#define VAH_ERR_TOO_LARGE (-6)  /* request exceeds a stated maximum */
+
+/* ---- physics variants (reference compile-time macros, DynamicalVariables.h:13-15) ---- */
+#define VAH_IDEAL 0       /* N_q = 5:  T^{tau mu}, P_L */
+#define VAH_PIMUNU 1      /* N_q = 15: + pi_perp^{mu nu} (-DPIMUNU) */
+#define VAH_PIMUNU_PI 2   /* N_q = 16: + bulk Pi (-DPIMUNU -DPI) */
+
+/* ---- equations of state ---- */
+#define VAH_EOS_CONFORMAL 0 /* reference EquationOfState.cpp with CONFORMAL_EOS (:78,113,144) */
+#define VAH_EOS_TABLE 1     /* tabulated crossover EoS (vah_eos_table_build) */
+
+/* ---- zeta/s ---- */
+#define VAH_ZETA_REFERENCE 0 /* SourceTerms.cpp:36-44 */
+#define VAH_ZETA_CROSSOVER 1 /* height 0.05 at T = 155 MeV, half-width 50 MeV */
+
+/* ---- storage precision ---- */
+#define VAH_FP64 0 /* state stored and updated in FP64 */
+#define VAH_FP32 1 /* state stored in FP32; inversion and reductions in FP64 */
+
+/* ---- face-flux evaluation ---- */
+#define VAH_FLUX_PER_CELL 0 /* each face evaluated by both neighbouring cells with that cell's
+                               Newton guess and fallback energy, as the reference does
+                               (FullyDiscreteKurganovTadmorScheme.cpp:179,183) */
+#define VAH_FLUX_SHARED 1   /* each face evaluated once (guess/fallback of the left cell) */
+
+/* ---- field ids (order of the reference's CONSERVED_VARIABLES, DynamicalVariables.h:47-75) ---- */
+#define VAH_F_TTT 0
+#define VAH_F_TTX 1
+#define VAH_F_TTY 2
+#define VAH_F_TTN 3
+#define VAH_F_PL 4
+#define VAH_F_PITT 5
+#define VAH_F_PITX 6
+#define VAH_F_PITY 7
+#define VAH_F_PITN 8
+#define VAH_F_PIXX 9
+#define VAH_F_PIXY 10
+#define VAH_F_PIXN 11
+#define VAH_F_PIYY 12
+#define VAH_F_PIYN 13
+#define VAH_F_PINN 14
+#define VAH_F_PI 15
+#define VAH_F_E 16
+#define VAH_F_P 17
+#define VAH_F_UT 18
+#define VAH_F_UX 19
+#define VAH_F_UY 20
+#define VAH_F_UN 21
+#define VAH_F_UPT 22 /* u at the previous time step ("up", DynamicalVariables.h:120) */
+#define VAH_F_UPX 23
+#define VAH_F_UPY 24
+#define VAH_F_UPN 25
+#define VAH_NUM_FIELDS 26
+
+/* ---- EoS table layout ---- */
+#define VAH_EOS_TABLE_N 4096
+#define VAH_EOS_TABLE_HEADER 8
+#define VAH_EOS_TABLE_LEN(n) (VAH_EOS_TABLE_HEADER + 3 * (size_t)(n))
+
+/* Lattice (rhic/include/LatticeParameters.h:17-31; ghost counts implied). */
+typedef struct vah_lattice {
+    int nx, ny, nz;
+    double dx, dy, dz;
+} vah_lattice;
+
+/* Hydro parameters (rhic/include/HydroParameters.h:15-21). */
+typedef struct vah_hydro {
+    double t0;                 /* initialProperTimePoint */
+    double eta_over_s;         /* shearViscosityToEntropyDensity */
+    double freezeout_T_GeV;    /* freezeoutTemperatureGeV */
+} vah_hydro;
+
+typedef struct vah_options {
+    int physics;    /* VAH_IDEAL / VAH_PIMUNU / VAH_PIMUNU_PI */
+    int eos;        /* VAH_EOS_* */
+    int zeta;       /* VAH_ZETA_* */
+    int precision;  /* VAH_FP64 / VAH_FP32 */
+    int flux;       /* VAH_FLUX_* */
+    int device;     /* CUDA device ordinal */
+    void *stream;   /* cudaStream_t to queue work on; NULL = library-owned stream */
+} vah_options;
+
+typedef struct vah_stats {
+    long long face_fallbacks; /* face inversions that took the fallback, last step */
+    long long cell_fallbacks; /* cell inversions that took the fallback, last step */
+    long long nan_cells;      /* cells where a NaN reached e or u, last step */
+    long long steps;          /* steps taken since creation */
+} vah_stats;
+
+typedef struct vah_event vah_event;
+
+/* Fill `out` (length VAH_EOS_TABLE_LEN(n)) with the tabulated crossover EoS:
+ * n nodes uniform in ln e, each holding p, T, c_s^2 (T in fm^-1, e and p in
+ * fm^-4). c_s^2(T) = 1/3 - (1/3 - 0.15)/(1 + (T/155 MeV)^4). No reference
+ * counterpart (the reference ships closed-form fits only,
+ * EquationOfState.cpp:31-201). */
+int vah_eos_table_build(int n, double *out, size_t out_len);
+
+/* Create an event: allocate its device state and bind physics options.
+ * Replaces allocateHostMemory/allocateDeviceMemory + the parameter structs
+ * (DynamicalVariables.cpp:33-196, DynamicalVariables.cu:202-392). eos_table
+ * is copied (VAH_EOS_TABLE only; may be NULL otherwise). */
+int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, const vah_options *opt,
+                     const double *eos_table, vah_event **out);
+int vah_event_destroy(vah_event *ev);
+
+/* Copy one field between host memory and the event (reference layout;
+ * with_ghosts = 1: full nc* array, 0: interior nx*ny*nz only). Replaces the
+ * host<->device copies of DynamicalVariables.cu:394-482. */
+int vah_event_set_field(vah_event *ev, int field, const double *host, int with_ghosts);
+int vah_event_get_field(vah_event *ev, int field, double *host, int with_ghosts);
+
+/* Primitives currently in the event (e, p, u, pi^{tau mu}, Pi and, if
+ * pl_from_field, P_L) -> conserved T^{tau mu}, P_L; up = u.
+ * setConservedVariables, DynamicalVariables.cpp:197-287 (pl_from_field = 0
+ * keeps its hard-coded P_L = 0.0154483 e). */
+int vah_event_set_conserved(vah_event *ev, double t, int pl_from_field);
+
+/* Initial state from an energy density (the reference's init sequence
+ * setInitialConditions -> setConservedVariables -> setGhostCells,
+ * HydroPlugin.cpp:184-190): e given on the interior (nx*ny*nz, x fastest),
+ * p = EoS(e), u = (1,0,0,0), pi^{mu nu} = 0, Pi = 0 (InitialConditions.cpp:
+ * 29-52, 122-162), P_L by pl_mode, up = u, then conserved variables and
+ * ghost layers. */
+#define VAH_PL_REFERENCE 0 /* P_L = 0.0154483 e (DynamicalVariables.cpp:246-248) */
+#define VAH_PL_ISOTROPIC 1 /* P_L = p */
+int vah_event_init_from_e(vah_event *ev, double t0, const double *e_interior, int pl_mode);
+
+/* Zero-gradient ghost layers (faces) of the current state:
+ * setGhostCells, DynamicalVariables.cpp:349-356. */
+int vah_event_set_ghost_cells(vah_event *ev);
+
+/* One Heun RK2 step from t with step dt followed by the q <-> Q swap:
+ * rungeKutta2 + setCurrentConservedVariables
+ * (FullyDiscreteKurganovTadmorScheme.cpp:738-792, DynamicalVariables.cpp:497-499;
+ * CUDA: twoStepRungeKutta, FullyDiscreteKurganovTadmorScheme.cu:121-157). */
+int vah_rk2_step(vah_event *ev, double t, double dt);
+
+/* nsteps steps from t0 (t_n = t0 + n dt, HydroPlugin.cpp:208-233). */
+int vah_run(vah_event *ev, double t0, double dt, int nsteps);
+
+/* Block until the event's queued work is done; reports VAH_ERR_NAN if a
+ * step produced a NaN. */
+int vah_event_sync(vah_event *ev);
+int vah_event_stats(vah_event *ev, vah_stats *out);
+
+/* Device time (ms) of the stage kernels launched since the last call, and
+ * how many launches; enabled by vah_event_set_timing(ev, 1). */
+int vah_event_set_timing(vah_event *ev, int on);
+int vah_event_kernel_time(vah_event *ev, double *ms, long long *launches);
+
+/* Host-buffer form of the reference CPU step: the caller's host arrays (the
+ * reference's process globals q, e, p, u, up; fields ordered by VAH_F_*,
+ * full ghosted layout) are copied in, stepped once on the GPU, and copied
+ * back. Drop-in for rungeKutta2 on host arrays
+ * (FullyDiscreteKurganovTadmorScheme.h:13-15). `fields` holds
+ * VAH_NUM_FIELDS pointers; unused physics slots may be NULL. */
+int vah_rk2_step_host(vah_event *ev, double t, double dt, double *const *fields);
+
+/* ---- initial energy-density generators (host, deterministic) ----
+ * Replace the reference's GSL/libc-rand generators (GlauberModel.cpp:19-108,
+ * MonteCarloGlauberModel.cpp:17-108, InitialConditions.cpp:196-292) with the
+ * workloads' own definitions. Transverse profiles are nx*ny, x fastest,
+ * centred like the reference grid (x_i = (i - (nx-1)/2) dx); each is scaled so
+ * its maximum is e_peak, then e_floor is added. */
+int vah_ic_optical_glauber(int nx, int ny, double dx, double dy, double b, double sigma_nn_fm2, int A,
+                           double ws_R, double ws_a, double x_coll, double e_peak, double e_floor, double *e_xy);
+int vah_ic_mc_glauber(int nx, int ny, double dx, double dy, double b, double sigma_nn_fm2, int A, double ws_R,
+                      double ws_a, double width, unsigned long long seed, double e_peak, double e_floor,
+                      double *e_xy, int *npart_out);
+/* f(eta) = 1 for |eta| < eta_flat, exp(-(|eta|-eta_flat)^2 / (2 sigma_eta^2)) beyond. */
+int vah_ic_longitudinal(int nz, double dz, double eta_flat, double sigma_eta, double *f_eta);
+
+/* Library version string. */
+const char *vah_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -18,7 +18,8 @@
  *
  * Table layout (shared with the product, see include/vah.h VAH_EOS_TABLE_*):
  *   tab[0] = n, tab[1] = ln e_0, tab[2] = 1/d(ln e), tab[3] = d(ln e),
- *   tab[4..7] reserved, then p[n], T[n], cs2[n].
+ *   tab[4] = e_0, tab[5] = ln e_{n-1}, tab[6] = e_{n-1}, tab[7] = 0,
+ *   then p[n], T[n], cs2[n].
  */
 #ifndef VO_EOS_H
 #define VO_EOS_H
@@ -73,9 +74,9 @@ static inline vo_eos_point vo_table_lookup(const double *tab, double e) {
     const double *P = tab + VO_EOS_HEADER;
     const double *T = P + n;
     const double *C = T + n;
-    double lne0 = tab[1], inv = tab[2], dl = tab[3];
+    double lne0 = tab[1], inv = tab[2];
     if (!(e > 0.0)) {
-        r.p = e * (P[0] / exp(lne0));
+        r.p = e * (P[0] / tab[4]);
         r.T = 0.0;
         r.cs2 = C[0];
         return r;
@@ -83,17 +84,14 @@ static inline vo_eos_point vo_table_lookup(const double *tab, double e) {
     double x = log(e);
     double f = (x - lne0) * inv;
     if (f <= 0.0) {
-        double e0 = exp(lne0);
-        r.p = e * (P[0] / e0);
+        r.p = e * (P[0] / tab[4]);
         r.T = T[0] * exp((3.0 / 23.0) * (x - lne0));
         r.cs2 = C[0];
         return r;
     }
     if (f >= (double)(n - 1)) {
-        double xl = lne0 + (double)(n - 1) * dl;
-        double el = exp(xl);
-        r.p = e * (P[n - 1] / el);
-        r.T = T[n - 1] * exp(0.25 * (x - xl));
+        r.p = e * (P[n - 1] / tab[6]);
+        r.T = T[n - 1] * exp(0.25 * (x - tab[5]));
         r.cs2 = C[n - 1];
         return r;
     }

@@ -1,0 +1,141 @@
+// tests/hostcheck/vah_hostcheck.cpp -- test harness: the library's per-cell
+// stage code (gpu-vah_b200/csrc/vah_stage.cuh) compiled for the host and driven
+// cell by cell with the same buffer rotation as vah_rk2_step in vah_api.cu.
+// It lets the tests check the device formulas against the CPU oracle without
+// a GPU. Not part of the library, and never loaded by it.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "vah.h"
+#include "vah_powf_exc.h"
+#include "vah_stage.cuh"
+
+namespace {
+
+struct HostEvent {
+    int nx, ny, nz, ncx, ncy, ncz, nq, physics;
+    size_t ncell;
+    double dx, dy, dz, etabar;
+    std::vector<double> store;
+    double *q[16], *qS[16], *ep[2][2], *u[4], *up[4], *uS[4];
+    int cur;
+    vah::Eos eos;
+    std::vector<double> tab;
+    unsigned long long counters[4];
+};
+
+template <int PHYS>
+void run_stage(const vah::StageArgs<double> &a) {
+    for (int k = 0; k < a.nz; ++k)
+        for (int j = 0; j < a.ny; ++j)
+            for (int i = 0; i < a.nx; ++i) {
+                if (a.nz > 1) vah::stage_cell<double, PHYS, true>(a, i + 2, j + 2, k + 2);
+                else vah::stage_cell<double, PHYS, false>(a, i + 2, j + 2, k + 2);
+            }
+}
+
+void stage(HostEvent *h, const vah::StageArgs<double> &a) {
+    if (h->physics == 0) run_stage<0>(a);
+    else if (h->physics == 1) run_stage<1>(a);
+    else run_stage<2>(a);
+}
+
+void common(HostEvent *h, vah::StageArgs<double> &a) {
+    std::memset(&a, 0, sizeof(a));
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->nz; a.ncx = h->ncx; a.ncy = h->ncy;
+    a.plane = (long long)h->ncx * h->ncy;
+    a.dx = h->dx; a.dy = h->dy; a.dz = h->dz; a.etabar = h->etabar;
+    a.eos = h->eos;
+    a.counters = h->counters;
+}
+
+}  // namespace
+
+extern "C" {
+
+void *hc_create(int nx, int ny, int nz, double dx, double dy, double dz, double etabar, int physics, int eos,
+                int zeta, const double *tab, const unsigned *exc, int nexc) {
+    HostEvent *h = new HostEvent();
+    h->nx = nx; h->ny = ny; h->nz = nz; h->ncx = nx + 4; h->ncy = ny + 4; h->ncz = nz + 4;
+    h->ncell = (size_t)h->ncx * h->ncy * h->ncz;
+    h->physics = physics;
+    h->nq = physics == 0 ? 5 : (physics == 1 ? 15 : 16);
+    h->dx = dx; h->dy = dy; h->dz = dz; h->etabar = etabar;
+    h->store.assign(h->ncell * (32 + 4 + 12), 0.0);
+    double *p = h->store.data();
+    for (int n = 0; n < 16; ++n) { h->q[n] = p; p += h->ncell; h->qS[n] = p; p += h->ncell; }
+    for (int b = 0; b < 2; ++b) for (int m = 0; m < 2; ++m) { h->ep[b][m] = p; p += h->ncell; }
+    for (int m = 0; m < 4; ++m) { h->u[m] = p; p += h->ncell; h->up[m] = p; p += h->ncell; h->uS[m] = p; p += h->ncell; }
+    h->cur = 0;
+    h->eos.kind = eos;
+    h->eos.zeta = zeta;
+    if (tab) {
+        int n = (int)tab[0];
+        h->tab.assign(tab, tab + VAH_EOS_TABLE_LEN(n));
+        h->eos.tab = h->tab.data();
+    } else {
+        h->eos.tab = nullptr;
+    }
+    if (nexc < 0) {  // use the library's libm-exception table
+        const std::vector<uint32_t> &t = vah::powf_quarter_exceptions();
+        h->eos.exc = t.data();
+        h->eos.nexc = (int)(t.size() / 2);
+    } else {
+        h->eos.exc = (const uint32_t *)exc;
+        h->eos.nexc = nexc;
+    }
+    std::memset(h->counters, 0, sizeof(h->counters));
+    return h;
+}
+
+void hc_destroy(void *p) { delete (HostEvent *)p; }
+
+double *hc_field(void *p, int id) {
+    HostEvent *h = (HostEvent *)p;
+    if (id < 16) return h->q[id];
+    if (id == VAH_F_E) return h->ep[h->cur][0];
+    if (id == VAH_F_P) return h->ep[h->cur][1];
+    if (id >= VAH_F_UT && id <= VAH_F_UN) return h->u[id - VAH_F_UT];
+    if (id >= VAH_F_UPT && id <= VAH_F_UPN) return h->up[id - VAH_F_UPT];
+    return nullptr;
+}
+
+void hc_set_conserved(void *p, double t, int pl_from_field) {
+    HostEvent *h = (HostEvent *)p;
+    for (int k = 0; k < h->nz; ++k)
+        for (int j = 0; j < h->ny; ++j)
+            for (int i = 0; i < h->nx; ++i) {
+                long long s = (i + 2) + (long long)h->ncx * ((j + 2) + (long long)h->ncy * (k + 2));
+                if (h->physics == 0) vah::set_conserved_cell<double, 0>(h->q, h->u, h->up, h->ep[h->cur][0], t, pl_from_field, s);
+                else if (h->physics == 1) vah::set_conserved_cell<double, 1>(h->q, h->u, h->up, h->ep[h->cur][0], t, pl_from_field, s);
+                else vah::set_conserved_cell<double, 2>(h->q, h->u, h->up, h->ep[h->cur][0], t, pl_from_field, s);
+            }
+}
+
+void hc_step(void *p, double t, double dt) {
+    HostEvent *h = (HostEvent *)p;
+    const int c = h->cur, o = 1 - c;
+    vah::StageArgs<double> a;
+    common(h, a);
+    a.t_src = t; a.t_inv = t + dt; a.dt = dt; a.stage2 = 0;
+    for (int n = 0; n < 16; ++n) { a.qin[n] = h->q[n]; a.qout[n] = h->qS[n]; }
+    for (int m = 0; m < 4; ++m) { a.uin[m] = h->u[m]; a.upin[m] = h->up[m]; a.guess[m] = h->u[m]; a.uout[m] = h->uS[m]; }
+    a.ein = h->ep[c][0]; a.pin = h->ep[c][1]; a.eout = h->ep[o][0]; a.pout = h->ep[o][1];
+    stage(h, a);
+    common(h, a);
+    a.t_src = t + dt; a.t_inv = t + dt; a.dt = dt; a.stage2 = 1;
+    for (int n = 0; n < 16; ++n) { a.qin[n] = h->qS[n]; a.qavg[n] = h->q[n]; a.qout[n] = h->q[n]; }
+    for (int m = 0; m < 4; ++m) { a.uin[m] = h->uS[m]; a.upin[m] = h->u[m]; a.guess[m] = h->u[m]; a.uout[m] = h->up[m]; }
+    a.ein = h->ep[o][0]; a.pin = h->ep[o][1]; a.eout = h->ep[c][0]; a.pout = h->ep[c][1];
+    stage(h, a);
+    for (int m = 0; m < 4; ++m) { double *tmp = h->u[m]; h->u[m] = h->up[m]; h->up[m] = tmp; }
+}
+
+void hc_counters(void *p, unsigned long long *out) {
+    HostEvent *h = (HostEvent *)p;
+    for (int k = 0; k < 3; ++k) out[k] = h->counters[k];
+}
+
+}  // extern "C"
