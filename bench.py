@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--impl", default="vah", choices=["vah", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--flux", default="per_cell", choices=["per_cell", "shared", "fused"],
+                    help="per_cell: reference face semantics, face+cell launches; fused: the same in one "
+                         "launch per stage; shared: each face evaluated once")
     return ap.parse_args()
 
 
@@ -233,7 +236,9 @@ def run_vah(args, rank, world, dist):
     table = vah.eos_table()
     e0 = initial_energy_density(vah, table, seed=1 + rank)
     ev = vah.Event(NX, NY, NZ, DX, DX, DZ, ETA_S, physics=vah.VAH_PIMUNU_PI, eos=vah.VAH_EOS_TABLE,
-                   zeta=vah.VAH_ZETA_CROSSOVER, table=table, t0=T0, device=local, stream=stream.cuda_stream)
+                   zeta=vah.VAH_ZETA_CROSSOVER, table=table, t0=T0, device=local, stream=stream.cuda_stream,
+                   flux={"per_cell": vah.VAH_FLUX_PER_CELL, "shared": vah.VAH_FLUX_SHARED,
+                         "fused": vah.VAH_FLUX_PER_CELL_FUSED}[args.flux])
     ev.init_from_e(T0, e0, vah.VAH_PL_ISOTROPIC)
     t = T0
     ev.run(t, DT, args.warmup)
@@ -298,17 +303,19 @@ def run_vah(args, rank, world, dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "cells": cells, "global_batch": world, "parallelism": "replicas",
-                       "l2": "inputs larger than L2 (state 0.55 GB per event)", "dt_fm": DT, "tau0_fm": T0},
+                       "l2": "inputs larger than L2 (state 0.55 GB per event)", "dt_fm": DT, "tau0_fm": T0,
+                       "faces": args.flux},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic_per_launch(cells),
                          "peak_kind": f"{peak_kind} copy bandwidth",
                          "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
-                         "kernel": "stage_kernel (one fused RK stage), average of the two stage launches",
-                         "avg_launch_ms": 1000 * avg_launch_s},
+                         "kernel": ("stage_kernel (one fused RK stage)" if args.flux == "fused"
+                                    else "one RK stage: face_kernel x3 + cell_kernel") + ", average over the two stages",
+                         "avg_stage_ms": 1000 * avg_launch_s},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
                     "path": "vah_rk2_step_host (pinned host state in, one step, state out)"},
-            "gpu_launches": launches,
+            "gpu_launches": launches * (1 if args.flux == "fused" else 4),
             "stats": {"face_fallbacks": stats.face_fallbacks, "cell_fallbacks": stats.cell_fallbacks,
                       "nan_cells": stats.nan_cells}}
     clk_summary = clk.summary()

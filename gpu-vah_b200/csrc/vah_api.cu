@@ -31,6 +31,8 @@ struct vah_event {
     double *ep[2][2];  // [buffer][0 = e, 1 = p]
     int cur;           // current (e, p) buffer
     double *u[4], *up[4], *uS[4];
+    double *H[3][16];  // face fluxes (VAH_FLUX_SHARED): scratch of the stage launches
+    double *HR[3][16];
     double *d_tab;
     uint32_t *d_exc;
     int nexc;
@@ -84,6 +86,11 @@ void free_all(vah_event *ev) {
         cudaFree(ev->up[m]);
         cudaFree(ev->uS[m]);
     }
+    for (int d = 0; d < 3; ++d)
+        for (int n = 0; n < 16; ++n) {
+            cudaFree(ev->H[d][n]);
+            cudaFree(ev->HR[d][n]);
+        }
     cudaFree(ev->d_tab);
     cudaFree(ev->d_exc);
     cudaFree(ev->d_counters);
@@ -115,6 +122,11 @@ void fill_common(const vah_event *ev, StageArgs<double> &a) {
     a.etabar = ev->hydro.eta_over_s;
     a.eos = make_eos(ev);
     a.counters = ev->d_counters;
+    for (int d = 0; d < 3; ++d)
+        for (int n = 0; n < 16; ++n) {
+            a.H[d][n] = ev->H[d][n];
+            a.HR[d][n] = ev->HR[d][n];
+        }
 }
 
 int timed_launch(vah_event *ev, const StageArgs<double> &a) {
@@ -131,7 +143,10 @@ int timed_launch(vah_event *ev, const StageArgs<double> &a) {
         ev->tev_used += 2;
         VAH_TRY(cudaEventRecord(pair[0], ev->stream));
     }
-    VAH_TRY(vah::launch_stage<double>(a, ev->opt.physics, ev->stream));
+    if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED)
+        VAH_TRY(vah::launch_stage<double>(a, ev->opt.physics, ev->stream));
+    else
+        VAH_TRY(vah::launch_stage_split<double>(a, ev->opt.physics, ev->opt.flux == VAH_FLUX_PER_CELL, ev->stream));
     if (pair) VAH_TRY(cudaEventRecord(pair[1], ev->stream));
     return VAH_OK;
 }
@@ -150,7 +165,8 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     if (opt->eos != VAH_EOS_CONFORMAL && opt->eos != VAH_EOS_TABLE) return VAH_ERR_ARG;
     if (opt->eos == VAH_EOS_TABLE && !eos_table) return VAH_ERR_ARG;
     if (opt->precision != VAH_FP64) return VAH_ERR_ARG;  // FP32 storage: separate entry
-    if (opt->flux != VAH_FLUX_PER_CELL) return VAH_ERR_ARG;
+    if (opt->flux != VAH_FLUX_PER_CELL && opt->flux != VAH_FLUX_SHARED && opt->flux != VAH_FLUX_PER_CELL_FUSED)
+        return VAH_ERR_ARG;
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return VAH_ERR_NODEVICE;
@@ -199,6 +215,12 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
         alloc(&ev->up[m]);
         alloc(&ev->uS[m]);
     }
+    if (opt->flux != VAH_FLUX_PER_CELL_FUSED)
+        for (int d = 0; d < (lat->nz > 1 ? 3 : 2); ++d)
+            for (int n = 0; n < ev->nq; ++n) {
+                alloc(&ev->H[d][n]);
+                if (opt->flux == VAH_FLUX_PER_CELL) alloc(&ev->HR[d][n]);
+            }
     if (rc == VAH_OK && cudaMalloc((void **)&ev->d_counters, 4 * sizeof(unsigned long long)) != cudaSuccess)
         rc = VAH_ERR_NOMEM;
     if (rc == VAH_OK) cudaMemset(ev->d_counters, 0, 4 * sizeof(unsigned long long));

@@ -22,6 +22,36 @@ __global__ void __launch_bounds__(kBX *kBY) stage_kernel(const StageArgs<S> a) {
     stage_cell<S, PHYS, IS3D>(a, i + 2, j + 2, k + 2);
 }
 
+// Faces at +1/2 of the ghosted cells along DIR that bound an interior cell:
+// left cell index 1 .. n along DIR (ghost layer 1 included), interior across.
+template <typename S, int PHYS, int DIR, bool EXACT>
+__global__ void __launch_bounds__(kBX *kBY) face_kernel(const StageArgs<S> a) {
+    const int ext0 = DIR == 0 ? a.nx + 1 : a.nx;
+    const int ext1 = DIR == 1 ? a.ny + 1 : a.ny;
+    const int ext2 = DIR == 2 ? a.nz + 1 : a.nz;
+    const int i = blockIdx.x * kBX + threadIdx.x;
+    const int r = blockIdx.y * kBY + threadIdx.y;
+    if (i >= ext0 || r >= ext1 * ext2) return;
+    const int j = r % ext1, k = r / ext1;
+    const int gi = i + (DIR == 0 ? 1 : 2), gj = j + (DIR == 1 ? 1 : 2), gk = k + (DIR == 2 ? 1 : 2);
+    const long long st = DIR == 0 ? 1 : (DIR == 1 ? (long long)a.ncx : a.plane);
+    const long long s = gi + (long long)a.ncx * gj + a.plane * gk;
+    const unsigned fails = face_compute<S, PHYS, EXACT>(a, s, DIR, st);
+    if (a.counters) {
+        if (fails & 255u) count_add(a.counters + 0, fails & 255u);
+        if (fails >> 8) count_add(a.counters + 2, 1ull);
+    }
+}
+
+template <typename S, int PHYS, bool IS3D, bool EXACT>
+__global__ void __launch_bounds__(kBX *kBY) cell_kernel(const StageArgs<S> a) {
+    const int i = blockIdx.x * kBX + threadIdx.x;
+    const int r = blockIdx.y * kBY + threadIdx.y;
+    if (i >= a.nx || r >= a.ny * a.nz) return;
+    const int j = r % a.ny, k = r / a.ny;
+    cell_compute<S, PHYS, IS3D, EXACT>(a, i + 2, j + 2, k + 2);
+}
+
 template <typename S, int PHYS>
 __global__ void set_conserved_kernel(const FieldSet<S> q, const FieldSet<S> u, const FieldSet<S> up, const S *e,
                                      int nx, int ny, int nz, double t, int pl_from_field) {
@@ -94,6 +124,22 @@ cudaError_t stage_dispatch(const StageArgs<S> &a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+template <typename S, int PHYS, bool EXACT>
+cudaError_t split_dispatch(const StageArgs<S> &a, cudaStream_t stream) {
+    dim3 block(kBX, kBY);
+    face_kernel<S, PHYS, 0, EXACT><<<dim3((a.nx + 1 + kBX - 1) / kBX, (a.ny * a.nz + kBY - 1) / kBY), block, 0, stream>>>(a);
+    face_kernel<S, PHYS, 1, EXACT><<<dim3((a.nx + kBX - 1) / kBX, ((a.ny + 1) * a.nz + kBY - 1) / kBY), block, 0, stream>>>(a);
+    if (a.nz > 1)
+        face_kernel<S, PHYS, 2, EXACT>
+            <<<dim3((a.nx + kBX - 1) / kBX, (a.ny * (a.nz + 1) + kBY - 1) / kBY), block, 0, stream>>>(a);
+    dim3 grid((a.nx + kBX - 1) / kBX, (a.ny * a.nz + kBY - 1) / kBY);
+    if (a.nz > 1)
+        cell_kernel<S, PHYS, true, EXACT><<<grid, block, 0, stream>>>(a);
+    else
+        cell_kernel<S, PHYS, false, EXACT><<<grid, block, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
 int grid_for(long long n, int block) {
     long long g = (n + block - 1) / block;
     if (g > 148 * 64) g = 148 * 64;
@@ -109,6 +155,17 @@ cudaError_t launch_stage(const StageArgs<S> &a, int physics, cudaStream_t stream
     case kIdeal: return stage_dispatch<S, kIdeal>(a, stream);
     case kPimunu: return stage_dispatch<S, kPimunu>(a, stream);
     case kPimunuPi: return stage_dispatch<S, kPimunuPi>(a, stream);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename S>
+cudaError_t launch_stage_split(const StageArgs<S> &a, int physics, bool exact, cudaStream_t stream) {
+    switch (physics) {
+    case kIdeal: return exact ? split_dispatch<S, kIdeal, true>(a, stream) : split_dispatch<S, kIdeal, false>(a, stream);
+    case kPimunu: return exact ? split_dispatch<S, kPimunu, true>(a, stream) : split_dispatch<S, kPimunu, false>(a, stream);
+    case kPimunuPi:
+        return exact ? split_dispatch<S, kPimunuPi, true>(a, stream) : split_dispatch<S, kPimunuPi, false>(a, stream);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -154,6 +211,7 @@ cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cud
 }
 
 template cudaError_t launch_stage<double>(const StageArgs<double> &, int, cudaStream_t);
+template cudaError_t launch_stage_split<double>(const StageArgs<double> &, int, bool, cudaStream_t);
 template cudaError_t launch_set_conserved<double>(const FieldSet<double> &, const FieldSet<double> &,
                                                   const FieldSet<double> &, const double *, int, int, int, int,
                                                   double, int, cudaStream_t);

@@ -11,6 +11,12 @@ namespace vah {
 template <typename S>
 cudaError_t launch_stage(const StageArgs<S> &a, int physics, cudaStream_t stream);
 
+// One RK stage on the face/cell split: face launches (x, y[, z]) then the
+// cell launch; a.H (and a.HR when exact) must point at the face buffers.
+// exact = the reference's per-cell face evaluation.
+template <typename S>
+cudaError_t launch_stage_split(const StageArgs<S> &a, int physics, bool exact, cudaStream_t stream);
+
 // A set of device field pointers, passed to kernels by value.
 template <typename S>
 struct FieldSet {

@@ -37,6 +37,11 @@ struct StageArgs {
     S *eout, *pout;
     Eos eos;
     unsigned long long *counters;  // [face fallbacks, cell fallbacks, NaN cells]
+    // face/cell split: flux through the face at +1/2 of ghosted cell s along
+    // axis d, field n, as cell s evaluates it (H) and as cell s+1 does (HR,
+    // reference face semantics only); scratch of ncell entries per field
+    S *H[3][16];
+    S *HR[3][16];
 };
 
 VAH_HD void count_add(unsigned long long *c, unsigned long long v) {
@@ -183,6 +188,104 @@ VAH_HD void stage_cell(const StageArgs<S> &a, int i, int j, int k) {
 
     store_cell(a, s, NQ, val, u, e, p);
     // face ghost layers (setGhostCellsKernelI/J/K, DynamicalVariables.cpp:400-489)
+    const long long sy = a.ncx, sz = a.plane;
+    if (i == 2) { store_cell(a, s - 1, NQ, val, u, e, p); store_cell(a, s - 2, NQ, val, u, e, p); }
+    if (i == a.nx + 1) { store_cell(a, s + 1, NQ, val, u, e, p); store_cell(a, s + 2, NQ, val, u, e, p); }
+    if (j == 2) { store_cell(a, s - sy, NQ, val, u, e, p); store_cell(a, s - 2 * sy, NQ, val, u, e, p); }
+    if (j == a.ny + 1) { store_cell(a, s + sy, NQ, val, u, e, p); store_cell(a, s + 2 * sy, NQ, val, u, e, p); }
+    if (k == 2) { store_cell(a, s - sz, NQ, val, u, e, p); store_cell(a, s - 2 * sz, NQ, val, u, e, p); }
+    if (k == a.nz + 1) { store_cell(a, s + sz, NQ, val, u, e, p); store_cell(a, s + 2 * sz, NQ, val, u, e, p); }
+}
+
+// ------------------------------------------------------- face/cell split --
+// The face fluxes of a stage are computed by their own launch (face_compute)
+// into scratch buffers, and the cell launch (cell_compute) takes flux
+// differences from them. Two face modes:
+//   EXACT (reference semantics, VAH_FLUX_PER_CELL): the reference evaluates
+//     each face twice, once from each neighbour, with that neighbour's Newton
+//     guess and fallback energy (FullyDiscreteKurganovTadmorScheme.cpp:179,183);
+//     face_compute does the same, sharing the reconstruction: H[d][n][s] is
+//     the face at +1/2 of cell s as cell s evaluates it, HR[d][n][s] as cell
+//     s+1 evaluates it.
+//   shared (VAH_FLUX_SHARED): one evaluation per face with the left cell's
+//     guess and energy. Converged inversions agree with the reference to the
+//     solver tolerance squared; where the reference's inversion falls back
+//     (dilute edges), shared faces do not reproduce it.
+
+// Face at +1/2 of ghosted cell s along axis dir (stride st).
+template <typename S, int PHYS, bool EXACT>
+VAH_HD unsigned face_compute(const StageArgs<S> &a, long long s, int dir, long long st) {
+    constexpr int NQ = Phys<PHYS>::NQ;
+    double qR[NQ], qL[NQ], H[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) {
+        const double qm = ld(a.qin[n], s - st), q0 = ld(a.qin[n], s), qp = ld(a.qin[n], s + st),
+                     qpp = ld(a.qin[n], s + 2 * st);
+        qR[n] = qp - approx_derivative(q0, qp, qpp) * 0.5;
+        qL[n] = q0 + approx_derivative(qm, q0, qp) * 0.5;
+    }
+    const double ux = ld(a.uin[1], s), uy = ld(a.uin[2], s);
+    unsigned fails = face_flux<PHYS>(a.eos, a.t_src, qR, qL, dir, ld(a.ein, s), sqrt(fabs(ux * ux + uy * uy)), H);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) a.H[dir][n][s] = (S)H[n];
+    if (EXACT) {
+        const double vx = ld(a.uin[1], s + st), vy = ld(a.uin[2], s + st);
+        fails += face_flux<PHYS>(a.eos, a.t_src, qR, qL, dir, ld(a.ein, s + st), sqrt(fabs(vx * vx + vy * vy)), H);
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) a.HR[dir][n][s] = (S)H[n];
+    }
+    return fails;
+}
+
+// One interior cell of the split path.
+template <typename S, int PHYS, bool IS3D, bool EXACT>
+VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
+    constexpr int NQ = Phys<PHYS>::NQ;
+    const long long s = i + (long long)a.ncx * j + a.plane * k;
+    double qc[NQ], val[NQ], Sv[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) qc[n] = ld(a.qin[n], s);
+    CellGrad g;
+    load_cell_grad<S, IS3D>(a, s, g);
+    int bad = cell_sources<PHYS>(a.eos, qc, g, a.t_src, a.dt, a.etabar, Sv);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) val[n] = qc[n] + a.dt * Sv[n];
+    const long long strides[3] = {1, a.ncx, a.plane};
+    const double hs[3] = {a.dx, a.dy, a.dz};
+    const double ucomp[3] = {g.ux, g.uy, g.un};
+#pragma unroll
+    for (int dir = 0; dir < (IS3D ? 3 : 2); ++dir) {
+        const long long st = strides[dir];
+        const double c = a.dt / hs[dir];
+        const S *const *Hm = EXACT ? a.HR[dir] : a.H[dir];  // face -1/2 as this cell evaluates it
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) val[n] += c * (ld(Hm[n], s - st) - ld(a.H[dir][n], s));
+        if (Phys<PHYS>::PIMUNU) {
+            double d[16];
+            const double f = 1 / hs[dir] / 2;
+#pragma unroll
+            for (int n = 5; n < NQ; ++n) d[n] = (ld(a.qin[n], s + st) - ld(a.qin[n], s - st)) * f;
+            double Sa[4];
+            axis_sources<PHYS>(d, dir, ucomp[dir], g.ut, a.t_src, Sa);
+#pragma unroll
+            for (int n = 0; n < 4; ++n) val[n] += a.dt * Sa[n];
+        }
+    }
+    if (a.stage2) {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) val[n] = (val[n] + ld(a.qavg[n], s)) * 0.5;
+    }
+    const double gx = ld(a.guess[1], s), gy = ld(a.guess[2], s);
+    double prim[6], qfull[16];
+#pragma unroll
+    for (int n = 0; n < 16; ++n) qfull[n] = n < NQ ? val[n] : 0.0;
+    const int st = invert<PHYS>(a.eos, a.t_inv, qfull, g.e, sqrt(fabs(gx * gx + gy * gy)), prim);
+    double e = prim[0], p = prim[1];
+    double u[4] = {prim[2], prim[3], prim[4], prim[5]};
+    regulate<PHYS>(a.t_inv, e, p, val, u);
+    if (st != 0 && a.counters) count_add(a.counters + 1, 1ull);
+    if ((bad || st == 2) && a.counters) count_add(a.counters + 2, 1ull);
+    store_cell(a, s, NQ, val, u, e, p);
     const long long sy = a.ncx, sz = a.plane;
     if (i == 2) { store_cell(a, s - 1, NQ, val, u, e, p); store_cell(a, s - 2, NQ, val, u, e, p); }
     if (i == a.nx + 1) { store_cell(a, s + 1, NQ, val, u, e, p); store_cell(a, s + 2, NQ, val, u, e, p); }

@@ -18,7 +18,7 @@ VAH_IDEAL, VAH_PIMUNU, VAH_PIMUNU_PI = 0, 1, 2
 VAH_EOS_CONFORMAL, VAH_EOS_TABLE = 0, 1
 VAH_ZETA_REFERENCE, VAH_ZETA_CROSSOVER = 0, 1
 VAH_FP64, VAH_FP32 = 0, 1
-VAH_FLUX_PER_CELL, VAH_FLUX_SHARED = 0, 1
+VAH_FLUX_PER_CELL, VAH_FLUX_SHARED, VAH_FLUX_PER_CELL_FUSED = 0, 1, 2
 VAH_PL_REFERENCE, VAH_PL_ISOTROPIC = 0, 1
 NUM_FIELDS = 26
 F_E, F_P, F_UT, F_UX, F_UY, F_UN = 16, 17, 18, 19, 20, 21

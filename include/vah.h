@@ -51,10 +51,16 @@ extern "C" {
 #define VAH_FP32 1 /* state stored in FP32; inversion and reductions in FP64 */
 
 /* ---- face-flux evaluation ---- */
-#define VAH_FLUX_PER_CELL 0 /* each face evaluated by both neighbouring cells with that cell's
-                               Newton guess and fallback energy, as the reference does
-                               (FullyDiscreteKurganovTadmorScheme.cpp:179,183) */
-#define VAH_FLUX_SHARED 1   /* each face evaluated once (guess/fallback of the left cell) */
+#define VAH_FLUX_PER_CELL 0       /* each face evaluated by both neighbouring cells with that cell's
+                                     Newton guess and fallback energy, as the reference does
+                                     (FullyDiscreteKurganovTadmorScheme.cpp:179,183); face and cell
+                                     launches per stage, face fluxes in scratch buffers */
+#define VAH_FLUX_SHARED 1         /* each face evaluated once, with the left cell's guess and fallback
+                                     energy: equal to the reference up to the Newton tolerance squared
+                                     where inversions converge; it does not reproduce the reference's
+                                     inversion fallbacks (dilute edges) */
+#define VAH_FLUX_PER_CELL_FUSED 2 /* reference face semantics in one fused launch per stage (no face
+                                     scratch; fewer launches, lower occupancy) */
 
 /* ---- field ids (order of the reference's CONSERVED_VARIABLES, DynamicalVariables.h:47-75) ---- */
 #define VAH_F_TTT 0

@@ -21,6 +21,9 @@ struct HostEvent {
     std::vector<double> store;
     double *q[16], *qS[16], *ep[2][2], *u[4], *up[4], *uS[4];
     int cur;
+    int shared;  // VAH_FLUX_SHARED: faces once, then cells
+    std::vector<double> hstore;
+    double *H[3][16], *HR[3][16];
     vah::Eos eos;
     std::vector<double> tab;
     unsigned long long counters[4];
@@ -36,7 +39,38 @@ void run_stage(const vah::StageArgs<double> &a) {
             }
 }
 
+template <int PHYS, bool EXACT>
+void run_stage_split(const vah::StageArgs<double> &a) {
+    const long long strides[3] = {1, a.ncx, a.plane};
+    for (int dir = 0; dir < (a.nz > 1 ? 3 : 2); ++dir)
+        for (int k = (dir == 2 ? 1 : 2); k < a.nz + 2; ++k)
+            for (int j = (dir == 1 ? 1 : 2); j < a.ny + 2; ++j)
+                for (int i = (dir == 0 ? 1 : 2); i < a.nx + 2; ++i) {
+                    unsigned f = vah::face_compute<double, PHYS, EXACT>(a, i + (long long)a.ncx * j + a.plane * k,
+                                                                          dir, strides[dir]);
+                    a.counters[0] += f & 255u;
+                }
+    for (int k = 0; k < a.nz; ++k)
+        for (int j = 0; j < a.ny; ++j)
+            for (int i = 0; i < a.nx; ++i) {
+                if (a.nz > 1) vah::cell_compute<double, PHYS, true, EXACT>(a, i + 2, j + 2, k + 2);
+                else vah::cell_compute<double, PHYS, false, EXACT>(a, i + 2, j + 2, k + 2);
+            }
+}
+
+template <int PHYS>
+void run_split(int mode, const vah::StageArgs<double> &a) {
+    if (mode == 1) run_stage_split<PHYS, true>(a);
+    else run_stage_split<PHYS, false>(a);
+}
+
 void stage(HostEvent *h, const vah::StageArgs<double> &a) {
+    if (h->shared) {  // 1: split with reference faces, 2: split with shared faces
+        if (h->physics == 0) run_split<0>(h->shared, a);
+        else if (h->physics == 1) run_split<1>(h->shared, a);
+        else run_split<2>(h->shared, a);
+        return;
+    }
     if (h->physics == 0) run_stage<0>(a);
     else if (h->physics == 1) run_stage<1>(a);
     else run_stage<2>(a);
@@ -49,6 +83,11 @@ void common(HostEvent *h, vah::StageArgs<double> &a) {
     a.dx = h->dx; a.dy = h->dy; a.dz = h->dz; a.etabar = h->etabar;
     a.eos = h->eos;
     a.counters = h->counters;
+    for (int d = 0; d < 3; ++d)
+        for (int n = 0; n < 16; ++n) {
+            a.H[d][n] = h->H[d][n];
+            a.HR[d][n] = h->HR[d][n];
+        }
 }
 
 }  // namespace
@@ -69,6 +108,13 @@ void *hc_create(int nx, int ny, int nz, double dx, double dy, double dz, double 
     for (int b = 0; b < 2; ++b) for (int m = 0; m < 2; ++m) { h->ep[b][m] = p; p += h->ncell; }
     for (int m = 0; m < 4; ++m) { h->u[m] = p; p += h->ncell; h->up[m] = p; p += h->ncell; h->uS[m] = p; p += h->ncell; }
     h->cur = 0;
+    h->shared = 0;
+    h->hstore.assign(h->ncell * 96, 0.0);
+    for (int d = 0; d < 3; ++d)
+        for (int n = 0; n < 16; ++n) {
+            h->H[d][n] = h->hstore.data() + h->ncell * (16 * d + n);
+            h->HR[d][n] = h->hstore.data() + h->ncell * (48 + 16 * d + n);
+        }
     h->eos.kind = eos;
     h->eos.zeta = zeta;
     if (tab) {
@@ -91,6 +137,8 @@ void *hc_create(int nx, int ny, int nz, double dx, double dy, double dz, double 
 }
 
 void hc_destroy(void *p) { delete (HostEvent *)p; }
+
+void hc_set_split(void *p, int mode) { ((HostEvent *)p)->shared = mode; }
 
 double *hc_field(void *p, int id) {
     HostEvent *h = (HostEvent *)p;

@@ -66,7 +66,7 @@ def conformal_workload(nx=61, ny=61):
     return g, e2
 
 
-def start_both(g, e_int, t0, pl_mode=1):
+def start_both(g, e_int, t0, pl_mode=1, flux=0):
     o = V.Oracle(g)
     full = np.zeros(g.shape)
     full[2:-2, 2:-2, 2:-2] = e_int.reshape(g.nz, g.ny, g.nx)
@@ -74,14 +74,19 @@ def start_both(g, e_int, t0, pl_mode=1):
     V.load_state(o, {V.E: full.ravel(), V.PP: p.ravel(), V.UT: np.ones(g.ncell), V.PL: p.ravel()})
     o.set_conserved(t0, pl_mode)
     o.set_ghost_cells()
-    ev = V.Event(g, t0=t0)
+    ev = V.Event(g, t0=t0, flux=flux)
     ev.init_from_e(t0, e_int, pl_mode)
     return o, ev
 
 
-def test_gpu_conformal_2d_200_steps_within_1e9():
+# reference face semantics: split face/cell launches (0) and the fused stage (2)
+FLUX = pytest.mark.parametrize("flux", [0, 2], ids=["split", "fused"])
+
+
+@FLUX
+def test_gpu_conformal_2d_200_steps_within_1e9(flux):
     g, e2 = conformal_workload()
-    o, ev = start_both(g, e2, 0.5)
+    o, ev = start_both(g, e2, 0.5, flux=flux)
     for fid in V.state_ids(g.physics):
         assert rel_err(g.interior(o.field(fid)), g.interior(ev.get_field(fid)), 1e-12) < 1e-13, fid
     dt = 0.02
@@ -95,7 +100,8 @@ def test_gpu_conformal_2d_200_steps_within_1e9():
     ev.close()
 
 
-def test_gpu_table_3d_bulk_within_1e9():
+@FLUX
+def test_gpu_table_3d_bulk_within_1e9(flux):
     """3+1D MC-Glauber slab with the tabulated EoS, shear + bulk, eta/s = 0.16."""
     tab = V.eos_table()
     nx, ny, nz = 25, 23, 9
@@ -105,13 +111,36 @@ def test_gpu_table_3d_bulk_within_1e9():
     exy, _ = V.product.mc_glauber(nx, ny, g.dx, g.dy, 7.0, seed=5, e_peak=e_peak)
     f = V.product.longitudinal(nz, g.dz)
     e3 = (f[:, None] * exy[None, :]).ravel()
-    o, ev = start_both(g, e3, 0.25)
+    o, ev = start_both(g, e3, 0.25, flux=flux)
     dt = 0.005
     o.run(0.25, dt, 40)
     ev.run(0.25, dt, 40)
     ev.sync()
     errs = {fid: rel_err(g.interior(o.field(fid)), g.interior(ev.get_field(fid)), 1e-12) for fid in KEY_FIELDS}
     assert max(errs.values()) < 1e-9, errs
+    ev.close()
+
+
+def test_gpu_shared_faces_match_oracle_where_inversions_converge():
+    """VAH_FLUX_SHARED evaluates each face once; on a state without inversion
+    fallbacks it equals the reference to the Newton tolerance squared."""
+    tab = V.eos_table()
+    g = V.Grid(24, 20, 10, 0.2, 0.2, 0.2, 0.16, physics="pimunu_pi", eos="table", zeta="crossover", table=tab)
+    f = V.smooth_initial_state(g, 0.5, amp=200.0, floor=1.0, flow=0.3)
+    o = V.Oracle(g)
+    V.load_state(o, f)
+    o.set_conserved(0.5, 1)
+    o.set_ghost_cells()
+    ev = V.Event(g, t0=0.5, flux=1)
+    upload(ev, g, {fid: o.field(fid).copy() for fid in V.state_ids(g.physics)})
+    for n in range(30):
+        o.step(0.5 + 0.01 * n, 0.01)
+        assert o.stats()[0] == 0
+    ev.run(0.5, 0.01, 30)
+    ev.sync()
+    assert ev.stats().face_fallbacks == 0
+    for fid in KEY_FIELDS:
+        assert rel_err(g.interior(o.field(fid)), g.interior(ev.get_field(fid)), 1e-12) < 1e-10, fid
     ev.close()
 
 

@@ -21,12 +21,13 @@ def field_scale(g, fid, arr):
     return m
 
 
+@pytest.mark.parametrize("split", [0, 1, 2], ids=["fused", "split_reference_faces", "split_shared_faces"])
 @pytest.mark.parametrize("physics,eos,shape,pi_amp,steps", CASES)
-def test_host_build_of_device_code_matches_oracle(physics, eos, shape, pi_amp, steps):
+def test_host_build_of_device_code_matches_oracle(physics, eos, shape, pi_amp, steps, split):
     table = V.eos_table() if eos == "table" else None
     g = V.Grid(*shape, 0.2, 0.2, 0.2, 0.2, physics=physics, eos=eos,
                zeta="crossover" if eos == "table" else "reference", table=table)
-    o, h = V.Oracle(g), V.HostCheck(g)
+    o, h = V.Oracle(g), V.HostCheck(g, split=split)
     f = V.smooth_initial_state(g, 0.5, pi_amp=pi_amp)
     V.load_state(o, f)
     V.load_state(h, f)

@@ -205,14 +205,17 @@ def hostcheck_lib():
         L.hc_set_conserved.argtypes = [C.c_void_p, D, I]
         L.hc_step.argtypes = [C.c_void_p, D, D]
         L.hc_counters.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
+        L.hc_set_split.argtypes = [C.c_void_p, I]
         _hc = L
     return _hc
 
 
 class HostCheck:
-    def __init__(self, g: Grid, libm_exceptions=True):
+    def __init__(self, g: Grid, libm_exceptions=True, split=0):
         """libm_exceptions: reproduce the host libm's powf rounding in the
-        conformal temperature (as the library does) or not."""
+        conformal temperature (as the library does) or not. split: 0 = fused
+        per-cell stage, 1 = face/cell split with reference faces, 2 = split
+        with shared faces."""
         self.g = g
         self.L = hostcheck_lib()
         tab = g.table.ctypes.data_as(P) if g.table is not None else None
@@ -220,6 +223,7 @@ class HostCheck:
         nexc = -1 if libm_exceptions else 0
         self.h = self.L.hc_create(g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, g.etabar, g.physics, g.eos, g.zeta, tab, excp,
                                   nexc)
+        self.L.hc_set_split(self.h, int(split))
 
     def __del__(self):
         try:
