@@ -27,12 +27,13 @@ struct vah_event {
     size_t ncell;
     cudaStream_t stream;
     bool own_stream;
-    double *q[16], *qS[16];
-    double *ep[2][2];  // [buffer][0 = e, 1 = p]
+    size_t elem;       // bytes per stored value: 8 (VAH_FP64) or 4 (VAH_FP32)
+    void *q[16], *qS[16];
+    void *ep[2][2];    // [buffer][0 = e, 1 = p]
     int cur;           // current (e, p) buffer
-    double *u[4], *up[4], *uS[4];
-    double *H[3][16];  // face fluxes (VAH_FLUX_SHARED): scratch of the stage launches
-    double *HR[3][16];
+    void *u[4], *up[4], *uS[4];
+    void *H[3][16];    // face fluxes as the left cell evaluates them (scratch of a stage)
+    void *HR[3][16];   // ... and as the right cell does (reference face semantics)
     double *d_tab;
     uint32_t *d_exc;
     int nexc;
@@ -63,7 +64,7 @@ int cuda_status(cudaError_t e) {
         if (e_ != cudaSuccess) return cuda_status(e_); \
     } while (0)
 
-double *field_ptr(vah_event *ev, int id) {
+void *field_ptr(vah_event *ev, int id) {
     if (id >= 0 && id < 16) return ev->q[id];  // null for slots the physics variant lacks
     switch (id) {
     case VAH_F_E: return ev->ep[ev->cur][0];
@@ -108,7 +109,8 @@ vah::Eos make_eos(const vah_event *ev) {
     return eos;
 }
 
-void fill_common(const vah_event *ev, StageArgs<double> &a) {
+template <typename S>
+void fill_common(const vah_event *ev, StageArgs<S> &a) {
     memset(&a, 0, sizeof(a));
     a.nx = ev->lat.nx;
     a.ny = ev->lat.ny;
@@ -124,12 +126,13 @@ void fill_common(const vah_event *ev, StageArgs<double> &a) {
     a.counters = ev->d_counters;
     for (int d = 0; d < 3; ++d)
         for (int n = 0; n < 16; ++n) {
-            a.H[d][n] = ev->H[d][n];
-            a.HR[d][n] = ev->HR[d][n];
+            a.H[d][n] = (S *)ev->H[d][n];
+            a.HR[d][n] = (S *)ev->HR[d][n];
         }
 }
 
-int timed_launch(vah_event *ev, const StageArgs<double> &a) {
+template <typename S>
+int timed_launch(vah_event *ev, const StageArgs<S> &a) {
     cudaEvent_t *pair = nullptr;
     if (ev->timing) {
         if ((size_t)(ev->tev_used + 2) > ev->tev.size()) {
@@ -144,9 +147,9 @@ int timed_launch(vah_event *ev, const StageArgs<double> &a) {
         VAH_TRY(cudaEventRecord(pair[0], ev->stream));
     }
     if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED)
-        VAH_TRY(vah::launch_stage<double>(a, ev->opt.physics, ev->stream));
+        VAH_TRY(vah::launch_stage<S>(a, ev->opt.physics, ev->stream));
     else
-        VAH_TRY(vah::launch_stage_split<double>(a, ev->opt.physics, ev->opt.flux == VAH_FLUX_PER_CELL, ev->stream));
+        VAH_TRY(vah::launch_stage_split<S>(a, ev->opt.physics, ev->opt.flux == VAH_FLUX_PER_CELL, ev->stream));
     if (pair) VAH_TRY(cudaEventRecord(pair[1], ev->stream));
     return VAH_OK;
 }
@@ -164,7 +167,7 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     if (opt->physics < VAH_IDEAL || opt->physics > VAH_PIMUNU_PI) return VAH_ERR_ARG;
     if (opt->eos != VAH_EOS_CONFORMAL && opt->eos != VAH_EOS_TABLE) return VAH_ERR_ARG;
     if (opt->eos == VAH_EOS_TABLE && !eos_table) return VAH_ERR_ARG;
-    if (opt->precision != VAH_FP64) return VAH_ERR_ARG;  // FP32 storage: separate entry
+    if (opt->precision != VAH_FP64 && opt->precision != VAH_FP32) return VAH_ERR_ARG;
     if (opt->flux != VAH_FLUX_PER_CELL && opt->flux != VAH_FLUX_SHARED && opt->flux != VAH_FLUX_PER_CELL_FUSED)
         return VAH_ERR_ARG;
 
@@ -183,6 +186,7 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->ncy = lat->ny + 4;
     ev->ncz = lat->nz + 4;
     ev->ncell = (size_t)ev->ncx * ev->ncy * ev->ncz;
+    ev->elem = opt->precision == VAH_FP32 ? sizeof(float) : sizeof(double);
     ev->cur = 0;
     ev->tev_used = 0;
     ev->kernel_ms = 0;
@@ -192,10 +196,10 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->nexc = 0;
     ev->own_stream = opt->stream == nullptr;
     int rc = VAH_OK;
-    auto alloc = [&](double **p) {
+    auto alloc = [&](void **p) {
         if (rc != VAH_OK) return;
-        cudaError_t e = cudaMalloc((void **)p, ev->ncell * sizeof(double));
-        if (e == cudaSuccess) e = cudaMemset(*p, 0, ev->ncell * sizeof(double));
+        cudaError_t e = cudaMalloc(p, ev->ncell * ev->elem);
+        if (e == cudaSuccess) e = cudaMemset(*p, 0, ev->ncell * ev->elem);
         if (e != cudaSuccess) rc = cuda_status(e);
     };
     if (ev->own_stream) {
@@ -258,76 +262,120 @@ extern "C" int vah_event_destroy(vah_event *ev) {
     return VAH_OK;
 }
 
-extern "C" int vah_event_set_field(vah_event *ev, int field, const double *host, int with_ghosts) {
-    if (!ev || !host) return VAH_ERR_ARG;
-    double *d = field_ptr(ev, field);
-    if (!d) return VAH_ERR_ARG;
-    VAH_TRY(cudaSetDevice(ev->opt.device));
-    if (with_ghosts) {
-        VAH_TRY(cudaMemcpyAsync(d, host, ev->ncell * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
-        VAH_TRY(cudaStreamSynchronize(ev->stream));
-        return VAH_OK;
-    }
-    // interior rows: one 2D copy per eta layer
+namespace {
+
+// Copy interior or full arrays between double host memory and the event's
+// storage type; FP32 storage converts through a host staging buffer.
+int copy_field(vah_event *ev, void *d, double *host_out, const double *host_in, int with_ghosts) {
     const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz;
-    for (int k = 0; k < nz; ++k) {
-        double *dst = d + 2 + (size_t)ev->ncx * (2 + (size_t)ev->ncy * (k + 2));
-        const double *src = host + (size_t)nx * ny * k;
-        VAH_TRY(cudaMemcpy2DAsync(dst, ev->ncx * sizeof(double), src, nx * sizeof(double), nx * sizeof(double), ny,
-                                  cudaMemcpyHostToDevice, ev->stream));
+    const size_t full = ev->ncell, inner = (size_t)nx * ny * nz;
+    const size_t n = with_ghosts ? full : inner;
+    const bool to_dev = host_in != nullptr;
+    std::vector<float> stage;
+    if (ev->elem == sizeof(float)) {
+        stage.resize(n);
+        if (to_dev)
+            for (size_t k = 0; k < n; ++k) stage[k] = (float)host_in[k];
+    }
+    const void *src_h = ev->elem == sizeof(float) ? (const void *)stage.data() : (const void *)host_in;
+    void *dst_h = ev->elem == sizeof(float) ? (void *)stage.data() : (void *)host_out;
+    const size_t es = ev->elem;
+    if (with_ghosts) {
+        if (to_dev) VAH_TRY(cudaMemcpyAsync(d, src_h, full * es, cudaMemcpyHostToDevice, ev->stream));
+        else VAH_TRY(cudaMemcpyAsync(dst_h, d, full * es, cudaMemcpyDeviceToHost, ev->stream));
+    } else {
+        for (int k = 0; k < nz; ++k) {
+            char *dev_row = (char *)d + es * (2 + (size_t)ev->ncx * (2 + (size_t)ev->ncy * (k + 2)));
+            const size_t off = es * (size_t)nx * ny * k;
+            if (to_dev)
+                VAH_TRY(cudaMemcpy2DAsync(dev_row, ev->ncx * es, (const char *)src_h + off, nx * es, nx * es, ny,
+                                          cudaMemcpyHostToDevice, ev->stream));
+            else
+                VAH_TRY(cudaMemcpy2DAsync((char *)dst_h + off, nx * es, dev_row, ev->ncx * es, nx * es, ny,
+                                          cudaMemcpyDeviceToHost, ev->stream));
+        }
     }
     VAH_TRY(cudaStreamSynchronize(ev->stream));
+    if (!to_dev && ev->elem == sizeof(float))
+        for (size_t k = 0; k < n; ++k) host_out[k] = (double)stage[k];
     return VAH_OK;
+}
+
+}  // namespace
+
+extern "C" int vah_event_set_field(vah_event *ev, int field, const double *host, int with_ghosts) {
+    if (!ev || !host) return VAH_ERR_ARG;
+    void *d = field_ptr(ev, field);
+    if (!d) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(ev->opt.device));
+    return copy_field(ev, d, nullptr, host, with_ghosts);
 }
 
 extern "C" int vah_event_get_field(vah_event *ev, int field, double *host, int with_ghosts) {
     if (!ev || !host) return VAH_ERR_ARG;
-    double *d = field_ptr(ev, field);
+    void *d = field_ptr(ev, field);
     if (!d) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(ev->opt.device));
-    if (with_ghosts) {
-        VAH_TRY(cudaMemcpyAsync(host, d, ev->ncell * sizeof(double), cudaMemcpyDeviceToHost, ev->stream));
-    } else {
-        const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz;
-        for (int k = 0; k < nz; ++k) {
-            const double *src = d + 2 + (size_t)ev->ncx * (2 + (size_t)ev->ncy * (k + 2));
-            double *dst = host + (size_t)nx * ny * k;
-            VAH_TRY(cudaMemcpy2DAsync(dst, nx * sizeof(double), src, ev->ncx * sizeof(double), nx * sizeof(double), ny,
-                                      cudaMemcpyDeviceToHost, ev->stream));
-        }
-    }
+    return copy_field(ev, d, host, nullptr, with_ghosts);
+}
+
+namespace {
+
+template <typename S>
+FieldSet<S> field_set(void *const *p, int n) {
+    FieldSet<S> f{};
+    for (int k = 0; k < n; ++k) f.f[k] = (S *)p[k];
+    f.n = n;
+    return f;
+}
+
+template <typename S>
+int set_conserved_t(vah_event *ev, double t, int pl_from_field) {
+    VAH_TRY(vah::launch_set_conserved<S>(field_set<S>(ev->q, 16), field_set<S>(ev->u, 4), field_set<S>(ev->up, 4),
+                                         (const S *)ev->ep[ev->cur][0], ev->opt.physics, ev->lat.nx, ev->lat.ny,
+                                         ev->lat.nz, t, pl_from_field, ev->stream));
     VAH_TRY(cudaStreamSynchronize(ev->stream));
     return VAH_OK;
 }
 
+template <typename S>
+int ghosts_t(vah_event *ev) {
+    FieldSet<S> f{};
+    int n = 0;
+    f.f[n++] = (S *)ev->ep[ev->cur][0];
+    f.f[n++] = (S *)ev->ep[ev->cur][1];
+    for (int m = 0; m < 4; ++m) f.f[n++] = (S *)ev->u[m];
+    for (int k = 0; k < 16; ++k)
+        if (ev->q[k]) f.f[n++] = (S *)ev->q[k];
+    f.n = n;
+    VAH_TRY(vah::launch_ghosts<S>(f, ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->stream));
+    VAH_TRY(cudaStreamSynchronize(ev->stream));
+    return VAH_OK;
+}
+
+template <typename S>
+int init_primitives_t(vah_event *ev) {
+    VAH_TRY(vah::launch_init_primitives<S>(field_set<S>(ev->q, 16), field_set<S>(ev->u, 4),
+                                           (const S *)ev->ep[ev->cur][0], (S *)ev->ep[ev->cur][1], make_eos(ev),
+                                           ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->stream));
+    return VAH_OK;
+}
+
+}  // namespace
+
 extern "C" int vah_event_set_conserved(vah_event *ev, double t, int pl_from_field) {
     if (!ev) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(ev->opt.device));
-    FieldSet<double> q{}, u{}, up{};
-    for (int n = 0; n < 16; ++n) q.f[n] = ev->q[n];
-    q.n = 16;
-    for (int m = 0; m < 4; ++m) {
-        u.f[m] = ev->u[m];
-        up.f[m] = ev->up[m];
-    }
-    u.n = up.n = 4;
-    VAH_TRY(vah::launch_set_conserved<double>(q, u, up, ev->ep[ev->cur][0], ev->opt.physics, ev->lat.nx, ev->lat.ny,
-                                              ev->lat.nz, t, pl_from_field, ev->stream));
-    VAH_TRY(cudaStreamSynchronize(ev->stream));
-    return VAH_OK;
+    return ev->elem == sizeof(float) ? set_conserved_t<float>(ev, t, pl_from_field)
+                                     : set_conserved_t<double>(ev, t, pl_from_field);
 }
 
 extern "C" int vah_event_init_from_e(vah_event *ev, double t0, const double *e_interior, int pl_mode) {
     if (!ev || !e_interior || (pl_mode != VAH_PL_REFERENCE && pl_mode != VAH_PL_ISOTROPIC)) return VAH_ERR_ARG;
     int rc = vah_event_set_field(ev, VAH_F_E, e_interior, 0);
     if (rc != VAH_OK) return rc;
-    FieldSet<double> q{}, u{};
-    for (int n = 0; n < 16; ++n) q.f[n] = ev->q[n];
-    q.n = 16;
-    for (int m = 0; m < 4; ++m) u.f[m] = ev->u[m];
-    u.n = 4;
-    VAH_TRY(vah::launch_init_primitives<double>(q, u, ev->ep[ev->cur][0], ev->ep[ev->cur][1], make_eos(ev),
-                                                ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->stream));
+    rc = ev->elem == sizeof(float) ? init_primitives_t<float>(ev) : init_primitives_t<double>(ev);
+    if (rc != VAH_OK) return rc;
     rc = vah_event_set_conserved(ev, t0, pl_mode == VAH_PL_ISOTROPIC);
     if (rc != VAH_OK) return rc;
     return vah_event_set_ghost_cells(ev);
@@ -336,24 +384,15 @@ extern "C" int vah_event_init_from_e(vah_event *ev, double t0, const double *e_i
 extern "C" int vah_event_set_ghost_cells(vah_event *ev) {
     if (!ev) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(ev->opt.device));
-    FieldSet<double> f{};
-    int n = 0;
-    f.f[n++] = ev->ep[ev->cur][0];
-    f.f[n++] = ev->ep[ev->cur][1];
-    for (int m = 0; m < 4; ++m) f.f[n++] = ev->u[m];
-    for (int k = 0; k < 16; ++k)
-        if (ev->q[k]) f.f[n++] = ev->q[k];
-    f.n = n;
-    VAH_TRY(vah::launch_ghosts<double>(f, ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->stream));
-    VAH_TRY(cudaStreamSynchronize(ev->stream));
-    return VAH_OK;
+    return ev->elem == sizeof(float) ? ghosts_t<float>(ev) : ghosts_t<double>(ev);
 }
 
-extern "C" int vah_rk2_step(vah_event *ev, double t, double dt) {
-    if (!ev || !(dt > 0) || !(t > 0)) return VAH_ERR_ARG;
-    VAH_TRY(cudaSetDevice(ev->opt.device));
+namespace {
+
+template <typename S>
+int rk2_step_t(vah_event *ev, double t, double dt) {
     const int c = ev->cur, o = 1 - ev->cur;
-    StageArgs<double> a;
+    StageArgs<S> a;
     // stage 1: q, u, (e, p)[c], up -> qS, uS, (e, p)[o]
     fill_common(ev, a);
     a.t_src = t;
@@ -361,19 +400,19 @@ extern "C" int vah_rk2_step(vah_event *ev, double t, double dt) {
     a.dt = dt;
     a.stage2 = 0;
     for (int n = 0; n < 16; ++n) {
-        a.qin[n] = ev->q[n];
-        a.qout[n] = ev->qS[n];
+        a.qin[n] = (const S *)ev->q[n];
+        a.qout[n] = (S *)ev->qS[n];
     }
     for (int m = 0; m < 4; ++m) {
-        a.uin[m] = ev->u[m];
-        a.upin[m] = ev->up[m];
-        a.guess[m] = ev->u[m];
-        a.uout[m] = ev->uS[m];
+        a.uin[m] = (const S *)ev->u[m];
+        a.upin[m] = (const S *)ev->up[m];
+        a.guess[m] = (const S *)ev->u[m];
+        a.uout[m] = (S *)ev->uS[m];
     }
-    a.ein = ev->ep[c][0];
-    a.pin = ev->ep[c][1];
-    a.eout = ev->ep[o][0];
-    a.pout = ev->ep[o][1];
+    a.ein = (const S *)ev->ep[c][0];
+    a.pin = (const S *)ev->ep[c][1];
+    a.eout = (S *)ev->ep[o][0];
+    a.pout = (S *)ev->ep[o][1];
     int rc = timed_launch(ev, a);
     if (rc != VAH_OK) return rc;
     // stage 2: qS, uS, (e, p)[o], u -> q (in place, with the convex
@@ -384,25 +423,33 @@ extern "C" int vah_rk2_step(vah_event *ev, double t, double dt) {
     a.dt = dt;
     a.stage2 = 1;
     for (int n = 0; n < 16; ++n) {
-        a.qin[n] = ev->qS[n];
-        a.qavg[n] = ev->q[n];
-        a.qout[n] = ev->q[n];
+        a.qin[n] = (const S *)ev->qS[n];
+        a.qavg[n] = (const S *)ev->q[n];
+        a.qout[n] = (S *)ev->q[n];
     }
     for (int m = 0; m < 4; ++m) {
-        a.uin[m] = ev->uS[m];
-        a.upin[m] = ev->u[m];
-        a.guess[m] = ev->u[m];
-        a.uout[m] = ev->up[m];
+        a.uin[m] = (const S *)ev->uS[m];
+        a.upin[m] = (const S *)ev->u[m];
+        a.guess[m] = (const S *)ev->u[m];
+        a.uout[m] = (S *)ev->up[m];
     }
-    a.ein = ev->ep[o][0];
-    a.pin = ev->ep[o][1];
-    a.eout = ev->ep[c][0];
-    a.pout = ev->ep[c][1];
-    rc = timed_launch(ev, a);
+    a.ein = (const S *)ev->ep[o][0];
+    a.pin = (const S *)ev->ep[o][1];
+    a.eout = (S *)ev->ep[c][0];
+    a.pout = (S *)ev->ep[c][1];
+    return timed_launch(ev, a);
+}
+
+}  // namespace
+
+extern "C" int vah_rk2_step(vah_event *ev, double t, double dt) {
+    if (!ev || !(dt > 0) || !(t > 0)) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(ev->opt.device));
+    int rc = ev->elem == sizeof(float) ? rk2_step_t<float>(ev, t, dt) : rk2_step_t<double>(ev, t, dt);
     if (rc != VAH_OK) return rc;
     // swapFluidVelocity(&up, &u) (FullyDiscreteKurganovTadmorScheme.cpp:784)
     for (int m = 0; m < 4; ++m) {
-        double *tmp = ev->u[m];
+        void *tmp = ev->u[m];
         ev->u[m] = ev->up[m];
         ev->up[m] = tmp;
     }
@@ -466,16 +513,27 @@ extern "C" int vah_event_kernel_time(vah_event *ev, double *ms, long long *launc
 extern "C" int vah_rk2_step_host(vah_event *ev, double t, double dt, double *const *fields) {
     if (!ev || !fields) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(ev->opt.device));
+    int rc;
+    if (ev->elem != sizeof(double)) {  // FP32 storage: converting copies
+        for (int id = 0; id < VAH_NUM_FIELDS; ++id)
+            if (field_ptr(ev, id) && fields[id] && (rc = vah_event_set_field(ev, id, fields[id], 1)) != VAH_OK)
+                return rc;
+        if ((rc = vah_rk2_step(ev, t, dt)) != VAH_OK || (rc = vah_event_sync(ev)) != VAH_OK) return rc;
+        for (int id = 0; id < VAH_NUM_FIELDS; ++id)
+            if (field_ptr(ev, id) && fields[id] && (rc = vah_event_get_field(ev, id, fields[id], 1)) != VAH_OK)
+                return rc;
+        return VAH_OK;
+    }
     const size_t bytes = ev->ncell * sizeof(double);
     // all copies are queued on the event's stream; one synchronisation at the end
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {
-        double *d = field_ptr(ev, id);
+        void *d = field_ptr(ev, id);
         if (d && fields[id]) VAH_TRY(cudaMemcpyAsync(d, fields[id], bytes, cudaMemcpyHostToDevice, ev->stream));
     }
-    int rc = vah_rk2_step(ev, t, dt);
+    rc = vah_rk2_step(ev, t, dt);
     if (rc != VAH_OK) return rc;
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {  // pointers after the u <-> up swap
-        double *d = field_ptr(ev, id);
+        void *d = field_ptr(ev, id);
         if (d && fields[id]) VAH_TRY(cudaMemcpyAsync(fields[id], d, bytes, cudaMemcpyDeviceToHost, ev->stream));
     }
     return vah_event_sync(ev);

@@ -210,14 +210,15 @@ cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cud
     return cudaSuccess;
 }
 
-template cudaError_t launch_stage<double>(const StageArgs<double> &, int, cudaStream_t);
-template cudaError_t launch_stage_split<double>(const StageArgs<double> &, int, bool, cudaStream_t);
-template cudaError_t launch_set_conserved<double>(const FieldSet<double> &, const FieldSet<double> &,
-                                                  const FieldSet<double> &, const double *, int, int, int, int,
-                                                  double, int, cudaStream_t);
-template cudaError_t launch_init_primitives<double>(const FieldSet<double> &, const FieldSet<double> &,
-                                                    const double *, double *, const Eos &, int, int, int,
-                                                    cudaStream_t);
-template cudaError_t launch_ghosts<double>(const FieldSet<double> &, int, int, int, cudaStream_t);
+#define VAH_INSTANTIATE(S)                                                                                      \
+    template cudaError_t launch_stage<S>(const StageArgs<S> &, int, cudaStream_t);                              \
+    template cudaError_t launch_stage_split<S>(const StageArgs<S> &, int, bool, cudaStream_t);                  \
+    template cudaError_t launch_set_conserved<S>(const FieldSet<S> &, const FieldSet<S> &, const FieldSet<S> &, \
+                                                 const S *, int, int, int, int, double, int, cudaStream_t);     \
+    template cudaError_t launch_init_primitives<S>(const FieldSet<S> &, const FieldSet<S> &, const S *, S *,    \
+                                                   const Eos &, int, int, int, cudaStream_t);                  \
+    template cudaError_t launch_ghosts<S>(const FieldSet<S> &, int, int, int, cudaStream_t);
+VAH_INSTANTIATE(double)
+VAH_INSTANTIATE(float)
 
 }  // namespace vah

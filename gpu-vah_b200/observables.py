@@ -1,0 +1,46 @@
+"""Event observables used to state the FP32 form's error against FP64.
+
+The reference defines none of these (SURVEY §7 hard part (v)); definitions:
+
+    E_tot(tau)  = sum over interior cells of tau * T^{tau tau} dx dy deta
+                  (the Milne energy; not conserved, it changes by
+                  -int tau P_L-like work terms, see tests)
+    eps_p(tau)  = sum (T^xx - T^yy) / sum (T^xx + T^yy)   (momentum anisotropy)
+    <u_T>(tau)  = sum e u^tau u_T / sum e u^tau           (energy-weighted flow)
+
+with T^xx = e (u^x)^2 + P_T (1 + (u^x)^2) + pi^xx (and likewise yy),
+P_T = (e - P_L - Rbar0(P_L/e)(e - 3p))/2 + 3/2 Pi. Sums run in float64 on the
+host over fields read back through the C ABI.
+"""
+import numpy as np
+
+RBAR0_NUM = [0.015267955823446243, 7.725572805021035, 421.0063884634789, 3422.877939650926, -5785.670846299543,
+             -12261.66452089229, 31491.409484673808, -22737.05146992673, 5441.373392185447]
+RBAR0_DEN = [0.05470696094814806, 14.505878005231883, 522.6643024173569, 2731.7776413939037, -6161.1991042880445,
+             -3989.4375208972588, 15008.260526258282, -10243.036679405379, 2116.74060159494]
+
+F_PL, F_PIXX, F_PIYY, F_PI = 4, 9, 12, 15
+F_TTT, F_E, F_P, F_UT, F_UX, F_UY = 0, 16, 17, 18, 19, 20
+
+
+def rbar0(a):
+    return np.polyval(RBAR0_NUM[::-1], a) / np.polyval(RBAR0_DEN[::-1], a)
+
+
+def observables(get, tau, dx, dy, dz, physics):
+    """get(field_id) -> interior array (float64)."""
+    e, p, pl = get(F_E), get(F_P), get(F_PL)
+    ut, ux, uy = get(F_UT), get(F_UX), get(F_UY)
+    bulk = get(F_PI) if physics == 2 else 0.0
+    pt = 0.5 * (e - pl - rbar0(pl / e) * (e - 3 * p)) + 1.5 * bulk
+    pixx = get(F_PIXX) if physics >= 1 else 0.0
+    piyy = get(F_PIYY) if physics >= 1 else 0.0
+    txx = e * ux ** 2 + pt * (1 + ux ** 2) + pixx
+    tyy = e * uy ** 2 + pt * (1 + uy ** 2) + piyy
+    uT = np.sqrt(ux ** 2 + uy ** 2)
+    w = e * ut
+    return {
+        "E_tot": float(np.sum(tau * get(F_TTT)) * dx * dy * dz),
+        "eps_p": float(np.sum(txx - tyy) / np.sum(txx + tyy)),
+        "uT_mean": float(np.sum(w * uT) / np.sum(w)),
+    }
