@@ -210,6 +210,44 @@ int vah_ic_mc_glauber(int nx, int ny, double dx, double dy, double b, double sig
 /* f(eta) = 1 for |eta| < eta_flat, exp(-(|eta|-eta_flat)^2 / (2 sigma_eta^2)) beyond. */
 int vah_ic_longitudinal(int nz, double dz, double eta_flat, double sigma_eta, double *f_eta);
 
+/* ---- one RK stage without allocation ----
+ * No counterpart in the reference: an entry point for callers that cannot
+ * allocate device memory (code inside a framework that owns all device memory
+ * through its own pool, work queued where cudaMalloc is not allowed or would
+ * synchronise the device, processes whose device footprint must stay fixed).
+ * It runs one RK stage -- the face/cell launches with the reference's face
+ * semantics, FP64 storage -- on state buffers the caller owns, and keeps the
+ * stage's scratch (face fluxes, fallback counters) in a fixed array of
+ * VAH_NOALLOC_SCRATCH_BYTES inside the library, held by every GPU that loads
+ * libvah.so until exit. It calls no allocator. Limit: 256 +
+ * (2 or 3 axes) * N_q * 2 * 8 bytes per ghosted cell must fit, i.e. at most
+ * 87,381 ghosted cells for a 3+1D grid with shear + bulk (N_q = 16) and
+ * 131,071 for a 2+1D one; larger grids return VAH_ERR_TOO_LARGE.
+ * The first call on a device looks up the array's device address (do it
+ * before any stream capture). Calls share the array: calls whose work
+ * overlaps on the GPU race on it. Stage 1 then stage 2 with the buffer roles
+ * of vah_rk2_step make one time step. The conformal temperature is the
+ * correctly rounded fourth root here (the host-libm correction table of the
+ * event path needs device memory). counts_out (host, 3 entries: face
+ * fallbacks, cell fallbacks, NaN cells; may be NULL) makes the call wait for
+ * the stage and returns VAH_ERR_NAN when a NaN reached e or u. */
+#define VAH_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+typedef struct vah_stage_buffers {
+    const double *q[16];     /* stage input conserved fields (VAH_F_* order; stage 1: q^n, stage 2: q*) */
+    const double *u[4];      /* stage input velocity (stage 1: u^n, stage 2: u*) */
+    const double *u_prev[4]; /* previous-stage velocity (stage 1: u^(n-1), stage 2: u^n); Newton guess in stage 2 */
+    const double *e, *p;     /* stage input e, p */
+    const double *q_avg[16]; /* stage 2: q^n for Q = (q^n + Q*)/2 (may alias q_out); unused in stage 1 */
+    double *q_out[16];       /* stage output conserved fields (interior and face ghost layers) */
+    double *u_out[4];
+    double *e_out, *p_out;
+} vah_stage_buffers;
+
+int vah_stage_noalloc(const vah_lattice *lat, double eta_over_s, int physics, int eos, int zeta,
+                      const double *d_eos_table, int stage, double t, double dt, const vah_stage_buffers *buf,
+                      void *stream, long long *counts_out);
+
 /* Library version string. */
 const char *vah_version(void);
 

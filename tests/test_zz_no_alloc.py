@@ -1,0 +1,116 @@
+"""vah_stage_noalloc: the RK stage for callers that cannot allocate device
+memory (framework-owned memory pools, contexts where cudaMalloc is not
+allowed, fixed device footprints). It keeps its face-flux scratch in a fixed
+array inside libvah.so, so here the test, playing such a caller, owns every
+state buffer (torch tensors) and the library allocates nothing. Two steps in
+a row -- four stage calls, the scratch reused between them -- must give what
+the allocating event path (vah_rk2_step) gives on the same state. The file
+sorts last so a run that stops at the first failure has run everything else."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import vahlib as V
+
+pytestmark = pytest.mark.gpu
+
+NQ = 16
+DP = C.POINTER(C.c_double)
+
+
+class StageBuffers(C.Structure):
+    _fields_ = [("q", DP * 16), ("u", DP * 4), ("u_prev", DP * 4), ("e", DP), ("p", DP), ("q_avg", DP * 16),
+                ("q_out", DP * 16), ("u_out", DP * 4), ("e_out", DP), ("p_out", DP)]
+
+
+def ptr(t):
+    return C.cast(C.c_void_p(t.data_ptr()), DP) if t is not None else DP()
+
+
+def noalloc_lib():
+    L = V.library()
+    L.vah_stage_noalloc.argtypes = [C.POINTER(V.product.Lattice), C.c_double, C.c_int, C.c_int, C.c_int, DP, C.c_int,
+                                    C.c_double, C.c_double, C.POINTER(StageBuffers), C.c_void_p,
+                                    C.POINTER(C.c_longlong)]
+    return L
+
+
+def rel_diff(got, ref):
+    d = np.max(np.abs(got - ref))
+    return 0.0 if d == 0 else d / np.max(np.abs(ref))
+
+
+def stage_call(L, lat, tab_dev, stage, t, dt, q, u, up, e, p, qavg, qo, uo, eo, po):
+    b = StageBuffers()
+    for n in range(NQ):
+        b.q[n] = ptr(q[n])
+        b.q_avg[n] = ptr(qavg[n]) if qavg is not None else DP()
+        b.q_out[n] = ptr(qo[n])
+    for m in range(4):
+        b.u[m], b.u_prev[m], b.u_out[m] = ptr(u[m]), ptr(up[m]), ptr(uo[m])
+    b.e, b.p, b.e_out, b.p_out = ptr(e), ptr(p), ptr(eo), ptr(po)
+    counts = (C.c_longlong * 3)()
+    rc = L.vah_stage_noalloc(C.byref(lat), 0.16, 2, 1, 1, ptr(tab_dev), stage, t, dt, C.byref(b), None, counts)
+    return rc, list(counts)
+
+
+def test_noalloc_stage_matches_event_step_twice():
+    import torch
+    torch.cuda.init()
+    L = noalloc_lib()
+    tab = V.eos_table()
+    nx, ny, nz = 24, 22, 9
+    g = V.Grid(nx, ny, nz, 0.3, 0.3, 0.1, 0.16, physics="pimunu_pi", eos="table", zeta="crossover", table=tab)
+    e_peak = V.product.table_energy_density(tab, 0.6 / 0.197326938)
+    exy, _ = V.product.mc_glauber(nx, ny, g.dx, g.dy, 6.0, seed=3, e_peak=e_peak)
+    ev = V.Event(g, t0=0.25, flux=0)
+    ev.init_from_e(0.25, (V.product.longitudinal(nz, g.dz)[:, None] * exy[None, :]).ravel(), 1)
+    ev.run(0.25, 0.005, 2)  # a state with flow and shear
+    ev.sync()
+
+    dev = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")
+    q = [dev(ev.get_field(n)) for n in range(NQ)]
+    e, p = dev(ev.get_field(V.E)), dev(ev.get_field(V.PP))
+    u = [dev(ev.get_field(V.UT + m)) for m in range(4)]
+    up = [dev(ev.get_field(V.UPT + m)) for m in range(4)]
+    qS = [torch.zeros_like(e) for _ in range(NQ)]
+    uS = [torch.zeros_like(e) for _ in range(4)]
+    e1, p1 = torch.zeros_like(e), torch.zeros_like(e)
+    tab_dev = dev(tab)
+    lat = V.product.Lattice(nx, ny, nz, g.dx, g.dy, g.dz)
+    torch.cuda.synchronize()
+
+    t, dt = 0.25 + 2 * 0.005, 0.005
+    for step in range(2):
+        rc, c1 = stage_call(L, lat, tab_dev, 1, t, dt, q, u, up, e, p, None, qS, uS, e1, p1)
+        assert rc == 0 and c1[2] == 0
+        # stage 2 writes q in place and u^{n+1} into the u^{n-1} buffer, as vah_rk2_step does
+        rc, c2 = stage_call(L, lat, tab_dev, 2, t, dt, qS, uS, u, e1, p1, q, q, up, e, p)
+        assert rc == 0 and c2[2] == 0
+        u, up = up, u
+        torch.cuda.synchronize()
+        ev.step(t, dt)
+        ev.sync()
+        pairs = [(fid, q[fid]) for fid in range(NQ)] + [(V.E, e), (V.PP, p)] + [(V.UT + m, u[m]) for m in range(4)]
+        for fid, arr in pairs:
+            assert rel_diff(arr.cpu().numpy(), ev.get_field(fid)) < 1e-12, (step, fid)
+        t += dt
+    ev.close()
+
+
+def test_noalloc_rejects_grids_beyond_its_scratch():
+    import torch
+    L = noalloc_lib()
+    big = V.product.Lattice(121, 121, 81, 0.1, 0.1, 0.1)
+    x = torch.zeros(8, dtype=torch.float64, device="cuda")
+    b = StageBuffers()
+    for n in range(NQ):
+        b.q[n] = b.q_avg[n] = b.q_out[n] = ptr(x)
+    for m in range(4):
+        b.u[m] = b.u_prev[m] = b.u_out[m] = ptr(x)
+    b.e = b.p = b.e_out = b.p_out = ptr(x)
+    rc = L.vah_stage_noalloc(C.byref(big), 0.16, 2, 1, 1, ptr(x), 1, 0.25, 0.005, C.byref(b), None, None)
+    assert rc == -6  # VAH_ERR_TOO_LARGE, nothing launched
+    rc = L.vah_stage_noalloc(C.byref(big), 0.16, 2, 1, 1, ptr(x), 3, 0.25, 0.005, C.byref(b), None, None)
+    assert rc == -1  # VAH_ERR_ARG (stage must be 1 or 2)
