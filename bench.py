@@ -45,6 +45,11 @@ def parse():
     ap.add_argument("--impl", default="vah", choices=["vah", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="event", choices=["event", "batch"],
+                    help="event: one 121x121x81 3+1D event; batch: 256 2+1D events of uneven size")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="fp32: state stored and updated in FP32, inversion in FP64")
+    ap.add_argument("--events", type=int, default=256)
     ap.add_argument("--flux", default="per_cell", choices=["per_cell", "shared", "fused"],
                     help="per_cell: reference face semantics, face+cell launches; fused: the same in one "
                          "launch per stage; shared: each face evaluated once")
@@ -226,6 +231,77 @@ def traffic_per_launch(cells):
     return d.get("dram_bytes_per_cell_per_launch", 0) * cells or None
 
 
+BATCH_SIDES = (81, 121, 161, 201)
+BATCH_DT = 0.01
+
+
+def batch_events(n, seed):
+    """The 2+1D batch: sides drawn from {81,121,161,201}, b uniform in [0,12] fm."""
+    rng = np.random.default_rng(seed)
+    return [(int(rng.choice(BATCH_SIDES)), float(rng.uniform(0, 12)), int(rng.integers(1, 2 ** 31))) for _ in range(n)]
+
+
+def run_batch(args, rank, world, dist):
+    import torch
+    import vah
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    table = vah.eos_table()
+    prec = vah.VAH_FP32 if args.precision == "fp32" else vah.VAH_FP64
+    flux = {"per_cell": vah.VAH_FLUX_PER_CELL, "shared": vah.VAH_FLUX_SHARED}[args.flux]
+    batch = vah.Batch(table=table, precision=prec, flux=flux, device=local, stream=stream.cuda_stream,
+                      capacity_bytes=150 << 30)
+    e_peak = vah.table_energy_density(table, 0.6 / vah.HBARC)
+    cells = 0
+    for side, b, seed in batch_events(args.events, 1000 + rank):
+        exy, _ = vah.mc_glauber(side, side, DX, DX, b, seed, e_peak=e_peak)
+        slot = batch.add(side, side, 1, DX, DX, DZ, T0, BATCH_DT, ETA_S, exy)
+        assert slot is not None, "batch capacity"
+        cells += side * side
+    batch.step(args.warmup)
+    batch.sync()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        batch.step(args.steps)
+        end.record(stream)
+        torch.cuda.synchronize()
+    elapsed = start.elapsed_time(end) / 1000.0
+    if dist is not None:
+        tt = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    batch.close()
+    if rank != 0:
+        return
+    w = 4 if prec == vah.VAH_FP32 else 8
+    bpc = (5 * NQ + 32) * w
+    value = world * cells * args.steps / elapsed
+    peak, peak_kind = measured_peaks()
+    achieved = bpc * cells * args.steps / elapsed / 1e9
+    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64-inversion" if prec == vah.VAH_FP32 else "f64", "data": "synthetic",
+            "config": {"workload": f"vah batch: {args.events} 2+1D MC-Glauber events, sides {BATCH_SIDES}, dx=0.1, "
+                                   f"b~U[0,12], table EoS, shear+bulk, dtau={BATCH_DT}",
+                       "events": args.events, "cells_per_step": cells, "faces": args.flux,
+                       "l2": "inputs larger than L2", "launch": "persistent tile work-list, CUDA graph per step"},
+            "events_step_per_s": world * args.events * args.steps / elapsed,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": f"{peak_kind} copy bandwidth",
+                         "algorithmic_bytes_per_cell_update": bpc, "kernel": "whole step (graph)"}}
+    s = clk.summary()
+    if s:
+        line["clocks"] = s
+    print(json.dumps(line), flush=True)
+
+
 def run_vah(args, rank, world, dist):
     import torch
     import vah
@@ -235,8 +311,10 @@ def run_vah(args, rank, world, dist):
     stream = torch.cuda.Stream()  # a real stream handle: the library queues its kernels on it
     table = vah.eos_table()
     e0 = initial_energy_density(vah, table, seed=1 + rank)
+    prec = vah.VAH_FP32 if args.precision == "fp32" else vah.VAH_FP64
     ev = vah.Event(NX, NY, NZ, DX, DX, DZ, ETA_S, physics=vah.VAH_PIMUNU_PI, eos=vah.VAH_EOS_TABLE,
                    zeta=vah.VAH_ZETA_CROSSOVER, table=table, t0=T0, device=local, stream=stream.cuda_stream,
+                   precision=prec,
                    flux={"per_cell": vah.VAH_FLUX_PER_CELL, "shared": vah.VAH_FLUX_SHARED,
                          "fused": vah.VAH_FLUX_PER_CELL_FUSED}[args.flux])
     ev.init_from_e(T0, e0, vah.VAH_PL_ISOTROPIC)
@@ -297,18 +375,21 @@ def run_vah(args, rank, world, dist):
         return
     peak, peak_kind = measured_peaks()
     avg_launch_s = kms / 1000.0 / max(launches, 1)
-    bytes_per_launch = BYTES_PER_CELL_UPDATE / 2 * cells
+    bpc = BYTES_PER_CELL_UPDATE if prec == vah.VAH_FP64 else BYTES_PER_CELL_UPDATE // 2
+    bytes_per_launch = bpc / 2 * cells
     achieved = bytes_per_launch / avg_launch_s / 1e9
     line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": cells, "global_batch": world, "parallelism": "replicas",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64-inversion" if prec == vah.VAH_FP32 else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD if prec == vah.VAH_FP64 else WORKLOAD.replace("FP64", "FP32 state"),
+                       "cells": cells, "global_batch": world, "parallelism": "replicas",
                        "l2": "inputs larger than L2 (state 0.55 GB per event)", "dt_fm": DT, "tau0_fm": T0,
                        "faces": args.flux},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic_per_launch(cells),
                          "peak_kind": f"{peak_kind} copy bandwidth",
-                         "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
+                         "algorithmic_bytes_per_cell_update": bpc,
                          "kernel": ("stage_kernel (one fused RK stage)" if args.flux == "fused"
                                     else "one RK stage: face_kernel x3 + cell_kernel") + ", average over the two stages",
                          "avg_stage_ms": 1000 * avg_launch_s},
@@ -346,6 +427,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "batch":
+            run_batch(args, rank, world, dist)
         else:
             run_vah(args, rank, world, dist)
     finally:

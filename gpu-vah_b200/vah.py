@@ -218,3 +218,115 @@ class Event:
         """Host-buffer step: ptrs = list of NUM_FIELDS host addresses (0 for unused)."""
         arr = (P * NUM_FIELDS)(*[C.cast(C.c_void_p(p), P) if p else P() for p in ptrs])
         check(self.L.vah_rk2_step_host(self.ev, t, dt, arr), "vah_rk2_step_host")
+
+
+class EventInfo(C.Structure):
+    _fields_ = [("t", D), ("steps", C.c_longlong), ("face_fallbacks", C.c_longlong),
+                ("cell_fallbacks", C.c_longlong), ("nan_cells", C.c_longlong), ("bytes", C.c_longlong)]
+
+
+VAH_ERR_FULL = -7
+
+
+def _batch_lib():
+    L = library()
+    if not getattr(L, "_batch_ready", False):
+        L.vah_batch_create.argtypes = [C.POINTER(Options), P, C.c_size_t, C.POINTER(C.c_void_p)]
+        for name in ("vah_batch_destroy", "vah_batch_sync"):
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.vah_batch_event_bytes.argtypes = [C.c_void_p, C.POINTER(Lattice), C.POINTER(C.c_size_t)]
+        L.vah_batch_add.argtypes = [C.c_void_p, C.POINTER(Lattice), C.POINTER(Hydro), D, P, I, C.POINTER(I)]
+        L.vah_batch_remove.argtypes = [C.c_void_p, I]
+        L.vah_batch_step.argtypes = [C.c_void_p, I]
+        L.vah_batch_event_info.argtypes = [C.c_void_p, I, C.POINTER(EventInfo)]
+        L.vah_batch_get_field.argtypes = [C.c_void_p, I, I, P, I]
+        L.vah_batch_max_energy_density.argtypes = [C.c_void_p, P, I]
+        L.vah_batch_observables.argtypes = [C.c_void_p, P, I]
+        L.vah_batch_set_timing.argtypes = [C.c_void_p, I]
+        L.vah_batch_kernel_time.argtypes = [C.c_void_p, P, C.POINTER(C.c_longlong)]
+        L._batch_ready = True
+    return L
+
+
+class Batch:
+    """Many device-resident events advanced together (vah_batch_*)."""
+
+    def __init__(self, physics=VAH_PIMUNU_PI, eos=VAH_EOS_TABLE, zeta=VAH_ZETA_CROSSOVER, table=None,
+                 capacity_bytes=64 << 30, precision=VAH_FP64, flux=VAH_FLUX_PER_CELL, device=0, stream=None):
+        self.L = _batch_lib()
+        self._table = None if table is None else np.ascontiguousarray(table, dtype=np.float64)
+        opt = Options(physics, eos, zeta, precision, flux, device, stream)
+        self.b = C.c_void_p()
+        tab = self._table.ctypes.data_as(P) if self._table is not None else None
+        check(self.L.vah_batch_create(C.byref(opt), tab, capacity_bytes, C.byref(self.b)), "vah_batch_create")
+        self.shapes = {}
+
+    def close(self):
+        if self.b:
+            self.L.vah_batch_destroy(self.b)
+            self.b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def event_bytes(self, nx, ny, nz):
+        n = C.c_size_t()
+        check(self.L.vah_batch_event_bytes(self.b, C.byref(Lattice(nx, ny, nz, 0.1, 0.1, 0.1)), C.byref(n)),
+              "vah_batch_event_bytes")
+        return n.value
+
+    def add(self, nx, ny, nz, dx, dy, dz, t0, dt, eta_over_s, e_interior, pl_mode=VAH_PL_ISOTROPIC):
+        """Returns the slot, or None when the batch is full (VAH_ERR_FULL)."""
+        a = np.ascontiguousarray(e_interior, dtype=np.float64)
+        slot = C.c_int()
+        rc = self.L.vah_batch_add(self.b, C.byref(Lattice(nx, ny, nz, dx, dy, dz)), C.byref(Hydro(t0, eta_over_s, 0.15)),
+                                  dt, a.ctypes.data_as(P), pl_mode, C.byref(slot))
+        if rc == VAH_ERR_FULL:
+            return None
+        check(rc, "vah_batch_add")
+        self.shapes[slot.value] = (nx, ny, nz)
+        return slot.value
+
+    def remove(self, slot):
+        check(self.L.vah_batch_remove(self.b, slot), "vah_batch_remove")
+        self.shapes.pop(slot, None)
+
+    def step(self, n=1):
+        check(self.L.vah_batch_step(self.b, n), "vah_batch_step")
+
+    def sync(self):
+        check(self.L.vah_batch_sync(self.b), "vah_batch_sync")
+
+    def info(self, slot):
+        i = EventInfo()
+        check(self.L.vah_batch_event_info(self.b, slot, C.byref(i)), "vah_batch_event_info")
+        return i
+
+    def get_field(self, slot, fid, with_ghosts=True):
+        nx, ny, nz = self.shapes[slot]
+        out = np.empty((nx + 4) * (ny + 4) * (nz + 4) if with_ghosts else nx * ny * nz)
+        check(self.L.vah_batch_get_field(self.b, slot, fid, out.ctypes.data_as(P), int(with_ghosts)),
+              "vah_batch_get_field")
+        return out
+
+    def max_energy_density(self, nslots):
+        out = np.zeros(nslots)
+        check(self.L.vah_batch_max_energy_density(self.b, out.ctypes.data_as(P), nslots),
+              "vah_batch_max_energy_density")
+        return out
+
+    def observables(self, nslots):
+        out = np.zeros(3 * nslots)
+        check(self.L.vah_batch_observables(self.b, out.ctypes.data_as(P), nslots), "vah_batch_observables")
+        return out.reshape(nslots, 3)
+
+    def set_timing(self, on):
+        check(self.L.vah_batch_set_timing(self.b, int(on)), "vah_batch_set_timing")
+
+    def kernel_time(self):
+        ms, n = D(), C.c_longlong()
+        check(self.L.vah_batch_kernel_time(self.b, C.byref(ms), C.byref(n)), "vah_batch_kernel_time")
+        return ms.value, n.value

@@ -32,6 +32,7 @@ extern "C" {
 #define VAH_ERR_NAN (-4)        /* a NaN reached e or u (reference: exit(-1)) */
 #define VAH_ERR_NODEVICE (-5)   /* no CUDA device / kernels not loadable */
 #define VAH_ERR_TOO_LARGE (-6)  /* request exceeds a stated maximum */
+#define VAH_ERR_FULL (-7)       /* batch capacity (bytes or slots) exhausted: retry after a removal */
 
 /* ---- physics variants (reference compile-time macros, DynamicalVariables.h:13-15) ---- */
 #define VAH_IDEAL 0       /* N_q = 5:  T^{tau mu}, P_L */
@@ -195,6 +196,55 @@ int vah_event_kernel_time(vah_event *ev, double *ms, long long *launches);
  * (FullyDiscreteKurganovTadmorScheme.h:13-15). `fields` holds
  * VAH_NUM_FIELDS pointers; unused physics slots may be NULL. */
 int vah_rk2_step_host(vah_event *ev, double t, double dt, double *const *fields);
+
+/* ---- batches: many events of uneven size in one launch per kernel kind ----
+ * No single reference counterpart: the reference advances one event per
+ * process (HydroPlugin.cpp:130-242). A batch keeps every admitted event's
+ * state device-resident and advances all of them together: each launch walks
+ * a work-list of 32x4-cell tiles over all events in a grid-stride loop, and
+ * one RK2 step of the whole batch (face and cell launches of both stages and
+ * the per-event clock advance) is replayed from a CUDA graph that is
+ * re-captured only when events are added or removed. Every event keeps its
+ * own time and dt; all share the batch's physics options (VAH_FLUX_PER_CELL
+ * or VAH_FLUX_SHARED). Admission is by device footprint: vah_batch_add
+ * returns VAH_ERR_FULL when the event would exceed capacity_bytes. */
+typedef struct vah_batch vah_batch;
+
+typedef struct vah_event_info {
+    double t;                 /* current proper time */
+    long long steps;          /* steps taken */
+    long long face_fallbacks; /* inversion fallbacks at faces since admission */
+    long long cell_fallbacks;
+    long long nan_cells;
+    long long bytes;          /* device footprint of the event */
+} vah_event_info;
+
+int vah_batch_create(const vah_options *opt, const double *eos_table, size_t capacity_bytes, vah_batch **out);
+int vah_batch_destroy(vah_batch *b);
+/* Device bytes an event of this lattice occupies in the batch. */
+int vah_batch_event_bytes(const vah_batch *b, const vah_lattice *lat, size_t *bytes);
+/* Admit an event: e on the interior (nx*ny*nz, x fastest) at hydro->t0, its
+ * own step dt; the vah_event_init_from_e initial state. */
+int vah_batch_add(vah_batch *b, const vah_lattice *lat, const vah_hydro *hydro, double dt, const double *e_interior,
+                  int pl_mode, int *slot);
+int vah_batch_remove(vah_batch *b, int slot);
+/* nsteps RK2 steps of every admitted event (asynchronous). */
+int vah_batch_step(vah_batch *b, int nsteps);
+int vah_batch_sync(vah_batch *b);
+int vah_batch_event_info(vah_batch *b, int slot, vah_event_info *out);
+int vah_batch_get_field(vah_batch *b, int slot, int field, double *host, int with_ghosts);
+/* Per-slot maximum energy density over the interior (the freeze-out test:
+ * max T < T_f with T monotone in e); out[s] = 0 for free slots. FP64,
+ * deterministic. */
+int vah_batch_max_energy_density(vah_batch *b, double *out, int nslots);
+/* Per-slot observables in FP64 with a fixed summation order (an event's
+ * values do not depend on the other events in the batch): out[3 s + 0] =
+ * sum tau T^{tau tau} dx dy deta, out[3 s + 1] = eps_p =
+ * sum(T^xx - T^yy)/sum(T^xx + T^yy), out[3 s + 2] = <u_T> = sum e u^tau u_T /
+ * sum e u^tau. */
+int vah_batch_observables(vah_batch *b, double *out, int nslots);
+int vah_batch_set_timing(vah_batch *b, int on);
+int vah_batch_kernel_time(vah_batch *b, double *ms, long long *steps);
 
 /* ---- initial energy-density generators (host, deterministic) ----
  * Replace the reference's GSL/libc-rand generators (GlauberModel.cpp:19-108,

@@ -1,0 +1,97 @@
+"""Batches (vah_batch_*): many uneven events in one launch per kernel kind,
+CUDA-graph steps, admission by footprint. An event's result must not depend
+on which other events share the batch."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import vahlib as V
+
+sys.path.insert(0, os.path.join(V.ROOT, "gpu-vah_b200"))
+import observables as OBS  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+vah = V.product
+
+
+def event_e(tab, nx, ny, nz, dx, dz, b, seed):
+    e_peak = vah.table_energy_density(tab, 0.5 / vah.HBARC)
+    exy, _ = vah.mc_glauber(nx, ny, dx, dx, b, seed, e_peak=e_peak)
+    return (vah.longitudinal(nz, dz)[:, None] * exy[None, :]).ravel()
+
+
+EVENTS = [(41, 37, 1, 0.3, 0.1, 4.0, 11, 0.01), (29, 33, 9, 0.4, 0.2, 6.0, 12, 0.008),
+          (64, 20, 1, 0.25, 0.1, 2.0, 13, 0.01), (18, 18, 6, 0.5, 0.3, 0.0, 14, 0.012)]
+
+
+@pytest.mark.parametrize("flux", [0, 1], ids=["reference_faces", "shared_faces"])
+def test_batch_equals_events_run_alone(flux):
+    tab = V.eos_table()
+    batch = vah.Batch(table=tab, flux=flux)
+    slots, alone = [], []
+    for (nx, ny, nz, dx, dz, b, seed, dt) in EVENTS:
+        e = event_e(tab, nx, ny, nz, dx, dz, b, seed)
+        slots.append(batch.add(nx, ny, nz, dx, dx, dz, 0.4, dt, 0.16, e))
+        ev = vah.Event(nx, ny, nz, dx, dx, dz, 0.16, table=tab, t0=0.4, flux=flux)
+        ev.init_from_e(0.4, e)
+        alone.append((ev, dt))
+    batch.step(7)
+    batch.sync()
+    for (ev, dt), slot, spec in zip(alone, slots, EVENTS):
+        ev.run(0.4, dt, 7)
+        ev.sync()
+        info = batch.info(slot)
+        assert info.steps == 7 and abs(info.t - (0.4 + 7 * dt)) < 1e-12
+        for fid in (0, 1, 2, 3, 4, 5, 9, 14, 15, 16, 17, 18, 19, 20, 21):
+            np.testing.assert_array_equal(batch.get_field(slot, fid, False), ev.get_field(fid, False),
+                                          err_msg=f"slot {slot} field {fid}")
+        ev.close()
+    batch.close()
+
+
+def test_batch_admission_removal_and_recapture():
+    tab = V.eos_table()
+    per = vah.Batch(table=tab).event_bytes(30, 30, 1)
+    batch = vah.Batch(table=tab, capacity_bytes=2 * per + per // 2)
+    e = event_e(tab, 30, 30, 1, 0.3, 0.1, 3.0, 21)
+    a = batch.add(30, 30, 1, 0.3, 0.3, 0.1, 0.4, 0.01, 0.16, e)
+    b = batch.add(30, 30, 1, 0.3, 0.3, 0.1, 0.4, 0.01, 0.16, e)
+    assert a is not None and b is not None
+    assert batch.add(30, 30, 1, 0.3, 0.3, 0.1, 0.4, 0.01, 0.16, e) is None  # over capacity: refused
+    batch.step(3)
+    batch.remove(a)
+    c = batch.add(30, 30, 1, 0.3, 0.3, 0.1, 0.4, 0.01, 0.16, e)  # admitted into the freed room, mid-run
+    assert c is not None
+    batch.step(3)
+    batch.sync()
+    assert batch.info(b).steps == 6 and batch.info(c).steps == 3
+    # c started later from the same state as b: after 3 steps c equals b after its first 3 steps
+    ref = vah.Event(30, 30, 1, 0.3, 0.3, 0.1, 0.16, table=tab, t0=0.4)
+    ref.init_from_e(0.4, e)
+    ref.run(0.4, 0.01, 3)
+    np.testing.assert_array_equal(batch.get_field(c, 16, False), ref.get_field(16, False))
+    ref.close()
+    batch.close()
+
+
+def test_batch_reductions_match_host():
+    tab = V.eos_table()
+    batch = vah.Batch(table=tab)
+    slots = []
+    for (nx, ny, nz, dx, dz, b, seed, dt) in EVENTS:
+        slots.append(batch.add(nx, ny, nz, dx, dx, dz, 0.4, dt, 0.16, event_e(tab, nx, ny, nz, dx, dz, b, seed)))
+    batch.step(5)
+    batch.sync()
+    n = max(slots) + 1
+    emax = batch.max_energy_density(n)
+    obs = batch.observables(n)
+    for slot, (nx, ny, nz, dx, dz, b, seed, dt) in zip(slots, EVENTS):
+        get = lambda f: batch.get_field(slot, f, False)
+        assert emax[slot] == np.max(get(16))
+        host = OBS.observables(get, 0.4 + 5 * dt, dx, dx, dz, 2)
+        assert abs(obs[slot, 0] / host["E_tot"] - 1) < 1e-12
+        assert abs(obs[slot, 1] - host["eps_p"]) < 1e-12 * max(1, abs(host["eps_p"]))
+        assert abs(obs[slot, 2] / host["uT_mean"] - 1) < 1e-12
+    batch.close()
