@@ -45,8 +45,10 @@ def parse():
     ap.add_argument("--impl", default="vah", choices=["vah", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="event", choices=["event", "batch"],
-                    help="event: one 121x121x81 3+1D event; batch: 256 2+1D events of uneven size")
+    ap.add_argument("--workload", default="event", choices=["event", "batch", "serve"],
+                    help="event: one 121x121x81 3+1D event; batch: 256 2+1D events of uneven size; "
+                         "serve: Poisson request stream served to freeze-out")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="serve: arrival window (s)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="fp32: state stored and updated in FP32, inversion in FP64")
     ap.add_argument("--events", type=int, default=256)
@@ -302,6 +304,26 @@ def run_batch(args, rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args, rank, world, dist):
+    import vah
+
+    if rank != 0:
+        return
+    prec = vah.VAH_FP32 if args.precision == "fp32" else vah.VAH_FP64
+    flux = {"per_cell": vah.VAH_FLUX_PER_CELL, "shared": vah.VAH_FLUX_SHARED}[args.flux]
+    res, lat = vah.serve(rate=50.0, duration_s=args.serve_seconds, seed=1, precision=prec, flux=flux,
+                         ic_threads=max(2, min(host_cores(), 32)))
+    line = {"metric": "events/s", "value": res["events_per_s"], "unit": "events/s", "n_gpus": 1,
+            "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64-inversion" if prec == vah.VAH_FP32 else "f64",
+            "data": "synthetic",
+            "config": {"workload": "vah serving: Poisson 50 events/s, 70% 2+1D side U[61,261], 30% 3+1D "
+                                   "81^2x41..161^2x81, b~U[0,14], dx=0.2, deta=0.2, dtau=0.02, freeze-out 150 MeV",
+                       "arrival_window_s": args.serve_seconds, "faces": args.flux},
+            "latency_p50_s": res["p50_s"], "latency_p99_s": res["p99_s"], "serve": res}
+    print(json.dumps(line), flush=True)
+
+
 def run_vah(args, rank, world, dist):
     import torch
     import vah
@@ -429,6 +451,8 @@ def main():
             run_reference(args, rank, world)
         elif args.workload == "batch":
             run_batch(args, rank, world, dist)
+        elif args.workload == "serve":
+            run_serve(args, rank, world, dist)
         else:
             run_vah(args, rank, world, dist)
     finally:

@@ -1,9 +1,10 @@
 // vah_batch.cu -- many events, one persistent launch per kernel kind.
 //
 // A batch holds up to kMaxSlots events of independent grid sizes. Every
-// launch of a step covers all events: its blocks walk a work-list of 32x4
-// tiles (event slot, tile origin) in a grid-stride loop, so events of uneven
-// sizes share one launch and the GPU is filled even by many small events.
+// launch of a step covers all events: a persistent grid of blocks walks a
+// work-list of 32x4 tiles (event slot, tile origin), each block a contiguous
+// run of it, so events of uneven sizes share one launch and the GPU is filled
+// even by many small events.
 // The per-event state lives in one device allocation per event (stream-
 // ordered, from the batch's memory pool); per-event descriptors (buffer
 // pointers, geometry) and clocks (time, u/u_prev parity, step count) live in
@@ -101,7 +102,11 @@ __global__ void __launch_bounds__(kTX *kTY) batch_kernel(const SlotDesc<S> *__re
     __shared__ int sa_slot;
     const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
     if (lead) sa_slot = -1;
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    // each block walks a contiguous run of the (slot-sorted) work-list, so the
+    // per-event arguments in shared memory change only at event boundaries
+    const int per = (nwork + gridDim.x - 1) / gridDim.x;
+    const int w0 = blockIdx.x * per, w1 = min(nwork, w0 + per);
+    for (int w = w0; w < w1; ++w) {
         const WorkItem it = work[w];
         __syncthreads();
         if (lead && it.slot != sa_slot) {

@@ -330,3 +330,36 @@ class Batch:
         ms, n = D(), C.c_longlong()
         check(self.L.vah_batch_kernel_time(self.b, C.byref(ms), C.byref(n)), "vah_batch_kernel_time")
         return ms.value, n.value
+
+
+class ServeConfig(C.Structure):
+    _fields_ = [("rate", D), ("duration_s", D), ("seed", C.c_ulonglong), ("frac_3d", D), ("side2_min", I),
+                ("side2_max", I), ("side3_min", I), ("side3_max", I), ("nz3_min", I), ("nz3_max", I), ("dx", D),
+                ("deta", D), ("b_max", D), ("t0", D), ("dt", D), ("eta_over_s", D), ("T0_GeV", D), ("Tf_GeV", D),
+                ("t_max", D), ("physics", I), ("eos", I), ("precision", I), ("flux", I), ("device", I),
+                ("capacity_bytes", C.c_size_t), ("chunk_steps", I), ("ic_threads", I)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("offered", C.c_longlong), ("completed", C.c_longlong), ("timeouts", C.c_longlong),
+                ("rejected", C.c_longlong), ("wall_s", D), ("events_per_s", D), ("p50_s", D), ("p99_s", D),
+                ("cell_updates", C.c_longlong), ("cell_updates_per_s", D), ("max_resident", C.c_longlong),
+                ("chunks", C.c_longlong)]
+
+
+def serve(**kw):
+    """Run the continuous-batching request loop (vah_serve_run); returns (result dict, latencies)."""
+    L = library()
+    L.vah_serve_run.argtypes = [C.POINTER(ServeConfig), C.POINTER(ServeResult), P, I]
+    cfg = dict(rate=50.0, duration_s=10.0, seed=1, frac_3d=0.3, side2_min=61, side2_max=261, side3_min=81,
+               side3_max=161, nz3_min=41, nz3_max=81, dx=0.2, deta=0.2, b_max=14.0, t0=0.25, dt=0.02,
+               eta_over_s=0.16, T0_GeV=0.6, Tf_GeV=0.150, t_max=40.0, physics=VAH_PIMUNU_PI, eos=VAH_EOS_TABLE,
+               precision=VAH_FP64, flux=VAH_FLUX_PER_CELL, device=0, capacity_bytes=120 << 30, chunk_steps=10,
+               ic_threads=16)
+    cfg.update(kw)
+    c = ServeConfig(**cfg)
+    r = ServeResult()
+    lat = np.zeros(100000)
+    check(L.vah_serve_run(C.byref(c), C.byref(r), lat.ctypes.data_as(P), lat.size), "vah_serve_run")
+    out = {k: getattr(r, k) for k, _ in ServeResult._fields_}
+    return out, lat[:r.completed].copy()

@@ -246,6 +246,42 @@ int vah_batch_observables(vah_batch *b, double *out, int nslots);
 int vah_batch_set_timing(vah_batch *b, int on);
 int vah_batch_kernel_time(vah_batch *b, double *ms, long long *steps);
 
+/* ---- serving: continuous batching of an open-loop request stream ----
+ * No reference counterpart (the reference runs one event per process). A
+ * seeded Poisson stream of requests (rate per second for duration_s; a
+ * fraction frac_3d are 3+1D with side and nz interpolated between the given
+ * bounds, the rest 2+1D with side uniform in [side2_min, side2_max]; impact
+ * parameter uniform in [0, b_max]; MC-Glauber initial conditions with peak
+ * temperature T0_GeV, built on ic_threads host threads at arrival) is served
+ * from one vah_batch: requests are admitted in arrival order while the batch
+ * has room (capacity_bytes), all resident events advance together in chunks
+ * of chunk_steps graph-replayed steps, and an event retires when its maximum
+ * temperature falls below Tf_GeV (FP64 device reduction after each chunk) or
+ * its time passes t_max (counted in timeouts). Latency = arrival to
+ * retirement, wall clock. latencies (optional) receives up to max_latencies
+ * values in completion order. */
+typedef struct vah_serve_config {
+    double rate, duration_s;
+    unsigned long long seed;
+    double frac_3d;
+    int side2_min, side2_max, side3_min, side3_max, nz3_min, nz3_max;
+    double dx, deta, b_max;
+    double t0, dt, eta_over_s, T0_GeV, Tf_GeV, t_max;
+    int physics, eos, precision, flux, device;
+    size_t capacity_bytes;
+    int chunk_steps, ic_threads;
+} vah_serve_config;
+
+typedef struct vah_serve_result {
+    long long offered, completed, timeouts, rejected;
+    double wall_s, events_per_s, p50_s, p99_s;
+    long long cell_updates;
+    double cell_updates_per_s;
+    long long max_resident, chunks;
+} vah_serve_result;
+
+int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res, double *latencies, int max_latencies);
+
 /* ---- initial energy-density generators (host, deterministic) ----
  * Replace the reference's GSL/libc-rand generators (GlauberModel.cpp:19-108,
  * MonteCarloGlauberModel.cpp:17-108, InitialConditions.cpp:196-292) with the

@@ -26,29 +26,48 @@ EVENTS = [(41, 37, 1, 0.3, 0.1, 4.0, 11, 0.01), (29, 33, 9, 0.4, 0.2, 6.0, 12, 0
           (64, 20, 1, 0.25, 0.1, 2.0, 13, 0.01), (18, 18, 6, 0.5, 0.3, 0.0, 14, 0.012)]
 
 
+FIELDS = (0, 1, 2, 3, 4, 5, 9, 14, 15, 16, 17, 18, 19, 20, 21)
+
+
+def rel(a, b, floor=0.0):
+    d = np.max(np.abs(a - b))
+    return 0.0 if d == 0 else d / max(np.max(np.abs(b)), floor)
+
+
 @pytest.mark.parametrize("flux", [0, 1], ids=["reference_faces", "shared_faces"])
-def test_batch_equals_events_run_alone(flux):
+def test_event_alone_and_in_the_mix_agree(flux):
+    """Each event gives bit-identical results alone in a batch and mixed with
+    the others (same kernels, per-event arithmetic only), and agrees with the
+    single-event path to 1e-12 (a separately compiled kernel: FMA contraction
+    may differ in the last bit)."""
     tab = V.eos_table()
-    batch = vah.Batch(table=tab, flux=flux)
-    slots, alone = [], []
+    mixed = vah.Batch(table=tab, flux=flux)
+    inputs = []
     for (nx, ny, nz, dx, dz, b, seed, dt) in EVENTS:
         e = event_e(tab, nx, ny, nz, dx, dz, b, seed)
-        slots.append(batch.add(nx, ny, nz, dx, dx, dz, 0.4, dt, 0.16, e))
+        inputs.append((mixed.add(nx, ny, nz, dx, dx, dz, 0.4, dt, 0.16, e), e))
+    mixed.step(7)
+    mixed.sync()
+    for (slot, e), (nx, ny, nz, dx, dz, b, seed, dt) in zip(inputs, EVENTS):
+        info = mixed.info(slot)
+        assert info.steps == 7 and abs(info.t - (0.4 + 7 * dt)) < 1e-12
+        alone = vah.Batch(table=tab, flux=flux)
+        s1 = alone.add(nx, ny, nz, dx, dx, dz, 0.4, dt, 0.16, e)
+        alone.step(7)
         ev = vah.Event(nx, ny, nz, dx, dx, dz, 0.16, table=tab, t0=0.4, flux=flux)
         ev.init_from_e(0.4, e)
-        alone.append((ev, dt))
-    batch.step(7)
-    batch.sync()
-    for (ev, dt), slot, spec in zip(alone, slots, EVENTS):
         ev.run(0.4, dt, 7)
         ev.sync()
-        info = batch.info(slot)
-        assert info.steps == 7 and abs(info.t - (0.4 + 7 * dt)) < 1e-12
-        for fid in (0, 1, 2, 3, 4, 5, 9, 14, 15, 16, 17, 18, 19, 20, 21):
-            np.testing.assert_array_equal(batch.get_field(slot, fid, False), ev.get_field(fid, False),
-                                          err_msg=f"slot {slot} field {fid}")
+        escale = np.max(mixed.get_field(slot, 16, False))
+        for fid in FIELDS:
+            got = mixed.get_field(slot, fid, False)
+            np.testing.assert_array_equal(got, alone.get_field(s1, fid, False), err_msg=f"slot {slot} field {fid}")
+            # pi components that vanish analytically in 2+1D carry roundoff only: floor at the e scale
+            floor = 1e-3 * escale if 5 <= fid <= 15 else 0.0
+            assert rel(got, ev.get_field(fid, False), floor) < 1e-12, (slot, fid)
         ev.close()
-    batch.close()
+        alone.close()
+    mixed.close()
 
 
 def test_batch_admission_removal_and_recapture():
@@ -67,11 +86,12 @@ def test_batch_admission_removal_and_recapture():
     batch.step(3)
     batch.sync()
     assert batch.info(b).steps == 6 and batch.info(c).steps == 3
-    # c started later from the same state as b: after 3 steps c equals b after its first 3 steps
-    ref = vah.Event(30, 30, 1, 0.3, 0.3, 0.1, 0.16, table=tab, t0=0.4)
-    ref.init_from_e(0.4, e)
-    ref.run(0.4, 0.01, 3)
-    np.testing.assert_array_equal(batch.get_field(c, 16, False), ref.get_field(16, False))
+    # c joined mid-run from the same state as b: after its 3 steps it equals a fresh 3-step run
+    ref = vah.Batch(table=tab)
+    r = ref.add(30, 30, 1, 0.3, 0.3, 0.1, 0.4, 0.01, 0.16, e)
+    ref.step(3)
+    for fid in FIELDS:
+        np.testing.assert_array_equal(batch.get_field(c, fid, False), ref.get_field(r, fid, False))
     ref.close()
     batch.close()
 
