@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
                     help="fp32: state stored and updated in FP32, inversion in FP64")
     ap.add_argument("--events", type=int, default=256)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the untuned launch configuration (the autotuner runs during warm-up otherwise)")
     ap.add_argument("--flux", default="per_cell", choices=["per_cell", "shared", "fused"],
                     help="per_cell: reference face semantics, face+cell launches; fused: the same in one "
                          "launch per stage; shared: each face evaluated once")
@@ -69,12 +71,13 @@ def measured_peaks():
 
 def initial_energy_density(vah, table, seed, nx=NX, ny=NY, nz=NZ):
     """MC-Glauber transverse profile x plateau+Gaussian longitudinal profile,
-    peak temperature 0.6 GeV under the tabulated EoS (interior, x fastest)."""
+    peak temperature 0.6 GeV under the tabulated EoS, plus 1e-3 fm^-4 after the
+    product as InitialConditions.cpp:247 adds it (interior, x fastest)."""
     e_peak = vah.table_energy_density(table, 0.6 / vah.HBARC)
-    exy, _ = vah.mc_glauber(nx, ny, DX, DX, B_IMPACT, seed, e_peak=e_peak)
+    exy, _ = vah.mc_glauber(nx, ny, DX, DX, B_IMPACT, seed, e_peak=e_peak, e_floor=0.0)
     f = vah.longitudinal(NZ, DZ)
     k0 = (NZ - nz) // 2
-    return np.ascontiguousarray((f[k0:k0 + nz, None] * exy[None, :]).ravel())
+    return np.ascontiguousarray((f[k0:k0 + nz, None] * exy[None, :]).ravel() + 1e-3)
 
 
 # ------------------------------------------------------------------ clocks --
@@ -264,6 +267,9 @@ def run_batch(args, rank, world, dist):
         cells += side * side
     batch.step(args.warmup)
     batch.sync()
+    tune = [] if args.no_autotune else batch.autotune(3)  # before the timed region; the state is unchanged
+    batch.step(1)  # re-capture the step graph with the chosen variants (untimed)
+    batch.sync()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -293,7 +299,8 @@ def run_batch(args, rank, world, dist):
             "config": {"workload": f"vah batch: {args.events} 2+1D MC-Glauber events, sides {BATCH_SIDES}, dx=0.1, "
                                    f"b~U[0,12], table EoS, shear+bulk, dtau={BATCH_DT}",
                        "events": args.events, "cells_per_step": cells, "faces": args.flux,
-                       "l2": "inputs larger than L2", "launch": "persistent tile work-list, CUDA graph per step"},
+                       "l2": "inputs larger than L2", "launch": "persistent tile work-list, CUDA graph per step",
+                       "autotune": {k: c for k, c in zip(("face_x", "face_y", "face_z", "cell_2d", "cell_3d"), tune)}},
             "events_step_per_s": world * args.events * args.steps / elapsed,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_kind": f"{peak_kind} copy bandwidth",
@@ -312,13 +319,15 @@ def run_serve(args, rank, world, dist):
     prec = vah.VAH_FP32 if args.precision == "fp32" else vah.VAH_FP64
     flux = {"per_cell": vah.VAH_FLUX_PER_CELL, "shared": vah.VAH_FLUX_SHARED}[args.flux]
     res, lat = vah.serve(rate=50.0, duration_s=args.serve_seconds, seed=1, precision=prec, flux=flux,
-                         ic_threads=max(2, min(host_cores(), 32)))
+                         T0_GeV=0.4, e_floor=1e-2, t_max=100.0, ic_threads=max(2, min(host_cores(), 32)))
     line = {"metric": "events/s", "value": res["events_per_s"], "unit": "events/s", "n_gpus": 1,
             "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64-inversion" if prec == vah.VAH_FP32 else "f64",
             "data": "synthetic",
             "config": {"workload": "vah serving: Poisson 50 events/s, 70% 2+1D side U[61,261], 30% 3+1D "
-                                   "81^2x41..161^2x81, b~U[0,14], dx=0.2, deta=0.2, dtau=0.02, freeze-out 150 MeV",
+                                   "81^2x41..161^2x81, b~U[0,14], dx=0.2, deta=0.2, dtau=0.02, MC-Glauber peak "
+                                   "T0=0.4 GeV + 0.01 fm^-4 floor, table EoS, eta/s=0.16, retired at max T<150 MeV "
+                                   "over converged cells (timeout tau=100 fm/c)",
                        "arrival_window_s": args.serve_seconds, "faces": args.flux},
             "latency_p50_s": res["p50_s"], "latency_p99_s": res["p99_s"], "serve": res}
     print(json.dumps(line), flush=True)
@@ -343,6 +352,8 @@ def run_vah(args, rank, world, dist):
     t = T0
     ev.run(t, DT, args.warmup)
     t += args.warmup * DT
+    ev.sync()
+    tune = [] if args.no_autotune else ev.autotune(3)  # before the timed region; the state is unchanged
     ev.sync()
 
     def barrier():
@@ -407,7 +418,8 @@ def run_vah(args, rank, world, dist):
             "config": {"workload": WORKLOAD if prec == vah.VAH_FP64 else WORKLOAD.replace("FP64", "FP32 state"),
                        "cells": cells, "global_batch": world, "parallelism": "replicas",
                        "l2": "inputs larger than L2 (state 0.55 GB per event)", "dt_fm": DT, "tau0_fm": T0,
-                       "faces": args.flux},
+                       "faces": args.flux,
+                       "autotune": {k: c for k, c in zip(("face_x", "face_y", "face_z", "cell"), tune)}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic_per_launch(cells),
                          "peak_kind": f"{peak_kind} copy bandwidth",

@@ -39,6 +39,8 @@ struct vah_event {
     int nexc;
     unsigned long long *d_counters;  // face fallbacks, cell fallbacks, NaN cells
     long long steps;
+    double last_t, last_dt;          // time and step of the latest vah_rk2_step (autotuning state)
+    vah::SplitConfig split;          // launch configuration of the face/cell kernels
     bool timing;
     std::vector<cudaEvent_t> tev;  // start/stop pairs of timed launches
     int tev_used;
@@ -149,7 +151,8 @@ int timed_launch(vah_event *ev, const StageArgs<S> &a) {
     if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED)
         VAH_TRY(vah::launch_stage<S>(a, ev->opt.physics, ev->stream));
     else
-        VAH_TRY(vah::launch_stage_split<S>(a, ev->opt.physics, ev->opt.flux == VAH_FLUX_PER_CELL, ev->stream));
+        VAH_TRY(vah::launch_stage_split<S>(a, ev->opt.physics, ev->opt.flux == VAH_FLUX_PER_CELL, ev->split,
+                                           ev->stream));
     if (pair) VAH_TRY(cudaEventRecord(pair[1], ev->stream));
     return VAH_OK;
 }
@@ -193,6 +196,9 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->kernel_launches = 0;
     ev->timing = false;
     ev->steps = 0;
+    ev->last_t = hydro->t0;
+    ev->last_dt = 0.005;
+    ev->split = vah::default_split_config();
     ev->nexc = 0;
     ev->own_stream = opt->stream == nullptr;
     int rc = VAH_OK;
@@ -389,11 +395,10 @@ extern "C" int vah_event_set_ghost_cells(vah_event *ev) {
 
 namespace {
 
+// Stage-1 arguments: q, u, (e, p)[cur], up -> qS, uS, (e, p)[1 - cur].
 template <typename S>
-int rk2_step_t(vah_event *ev, double t, double dt) {
+void stage1_args(const vah_event *ev, double t, double dt, StageArgs<S> &a) {
     const int c = ev->cur, o = 1 - ev->cur;
-    StageArgs<S> a;
-    // stage 1: q, u, (e, p)[c], up -> qS, uS, (e, p)[o]
     fill_common(ev, a);
     a.t_src = t;
     a.t_inv = t + dt;
@@ -413,6 +418,13 @@ int rk2_step_t(vah_event *ev, double t, double dt) {
     a.pin = (const S *)ev->ep[c][1];
     a.eout = (S *)ev->ep[o][0];
     a.pout = (S *)ev->ep[o][1];
+}
+
+template <typename S>
+int rk2_step_t(vah_event *ev, double t, double dt) {
+    const int c = ev->cur, o = 1 - ev->cur;
+    StageArgs<S> a;
+    stage1_args(ev, t, dt, a);
     int rc = timed_launch(ev, a);
     if (rc != VAH_OK) return rc;
     // stage 2: qS, uS, (e, p)[o], u -> q (in place, with the convex
@@ -454,7 +466,81 @@ extern "C" int vah_rk2_step(vah_event *ev, double t, double dt) {
         ev->up[m] = tmp;
     }
     ev->steps++;
+    ev->last_t = t + dt;
+    ev->last_dt = dt;
     return VAH_OK;
+}
+
+namespace {
+
+// Time every candidate launch configuration of each split kind on the
+// event's current state, in stage-1 buffer roles (their outputs -- the face
+// buffers, qS, uS and the other (e, p) pair -- are scratch that the next step
+// rewrites), and keep the fastest. The device counters are restored after.
+template <typename S>
+int autotune_t(vah_event *ev, int reps, vah_tune_report *out) {
+    StageArgs<S> a;
+    stage1_args(ev, ev->last_t, ev->last_dt, a);
+    const bool exact = ev->opt.flux == VAH_FLUX_PER_CELL;
+    unsigned long long saved[4];
+    VAH_TRY(cudaStreamSynchronize(ev->stream));
+    VAH_TRY(cudaMemcpy(saved, ev->d_counters, sizeof(saved), cudaMemcpyDeviceToHost));
+    cudaEvent_t e0, e1;
+    VAH_TRY(cudaEventCreate(&e0));
+    VAH_TRY(cudaEventCreate(&e1));
+    int rc = VAH_OK;
+    auto launch = [&](int kind, const vah::KindConfig &c) {
+        return vah::launch_split_kind<S>(a, ev->opt.physics, exact, kind, c, ev->stream);
+    };
+    auto time_one = [&](int kind, const vah::KindConfig &c, double *ms) -> int {
+        if (launch(kind, c) != cudaSuccess) return VAH_ERR_CUDA;  // warm-up
+        if (cudaEventRecord(e0, ev->stream) != cudaSuccess) return VAH_ERR_CUDA;
+        for (int r = 0; r < reps; ++r)
+            if (launch(kind, c) != cudaSuccess) return VAH_ERR_CUDA;
+        if (cudaEventRecord(e1, ev->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+            return VAH_ERR_CUDA;
+        float f = 0;
+        if (cudaEventElapsedTime(&f, e0, e1) != cudaSuccess) return VAH_ERR_CUDA;
+        *ms = f / reps;
+        return VAH_OK;
+    };
+    out->nkinds = vah::kNumSplitKinds;
+    for (int kind = 0; kind < vah::kNumSplitKinds && rc == VAH_OK; ++kind) {
+        vah_launch_choice &r = out->kind[kind];
+        const vah::KindConfig def = ev->split.k[kind];
+        r = {def.bx, def.by, def.minb, 0.0, 0.0};
+        if (kind == vah::kFaceZ && ev->lat.nz == 1) continue;  // no eta faces in 2+1D
+        vah::KindConfig cand[16];
+        const int n = vah::split_candidates(kind, cand, 16);
+        double best = 1e300;
+        for (int i = 0; i < n && rc == VAH_OK; ++i) {
+            double ms = 0;
+            rc = time_one(kind, cand[i], &ms);
+            if (rc != VAH_OK) break;
+            if (cand[i].bx == def.bx && cand[i].by == def.by && cand[i].minb == def.minb) r.ms_default = ms;
+            if (ms < best) {
+                best = ms;
+                ev->split.k[kind] = cand[i];
+            }
+        }
+        const vah::KindConfig &b = ev->split.k[kind];
+        r = {b.bx, b.by, b.minb, r.ms_default, best};
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cudaMemcpy(ev->d_counters, saved, sizeof(saved), cudaMemcpyHostToDevice) != cudaSuccess && rc == VAH_OK)
+        rc = VAH_ERR_CUDA;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int vah_event_autotune(vah_event *ev, int reps, vah_tune_report *out) {
+    if (!ev || !out || reps < 1) return VAH_ERR_ARG;
+    memset(out, 0, sizeof(*out));
+    if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED) return VAH_OK;  // one fused launch shape: nothing to tune
+    VAH_TRY(cudaSetDevice(ev->opt.device));
+    return ev->elem == sizeof(float) ? autotune_t<float>(ev, reps, out) : autotune_t<double>(ev, reps, out);
 }
 
 extern "C" int vah_run(vah_event *ev, double t0, double dt, int nsteps) {

@@ -34,6 +34,7 @@ struct SlotDesc {
     double dx, dy, dz, dt, etabar;
     S *q[16], *qS[16], *ep[2][2], *uA[4], *uB[4], *uS[4];
     S *H[3][16], *HR[3][16];
+    unsigned char *fallback;  // per ghosted cell: 1 where the latest cell inversion fell back
     unsigned long long *counters;
 };
 
@@ -69,6 +70,7 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
     a.stage2 = stage == 2;
     a.eos = eos;
     a.counters = d.counters;
+    a.fallback = d.fallback;
     S *const *u = c.parity ? d.uB : d.uA;
     S *const *up = c.parity ? d.uA : d.uB;
     for (int n = 0; n < 16; ++n) {
@@ -93,8 +95,8 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
         }
 }
 
-template <typename S, int PHYS, int KIND, bool EXACT>
-__global__ void __launch_bounds__(kTX *kTY) batch_kernel(const SlotDesc<S> *__restrict__ descs,
+template <typename S, int PHYS, int KIND, bool EXACT, int MINB>
+__global__ void __launch_bounds__(kTX *kTY, MINB) batch_kernel(const SlotDesc<S> *__restrict__ descs,
                                                          const SlotClock *__restrict__ clk,
                                                          const WorkItem *__restrict__ work, int nwork, int stage,
                                                          const Eos eos) {
@@ -144,8 +146,11 @@ __global__ void advance_kernel(SlotClock *clk, const double *dts, int nslots) {
     }
 }
 
-// Per-slot maximum of e over the interior (positive doubles order like their
-// bit patterns), for the freeze-out test. Order-independent, so deterministic.
+// Per-slot maximum of e over the interior cells whose latest inversion
+// converged (positive doubles order like their bit patterns), for the
+// freeze-out test. A cell whose inversion fell back holds e = 0.999 e_prev and
+// u = (1,0,0,0) instead of a solution, so it does not count. Order-
+// independent, so deterministic.
 template <typename S>
 __global__ void max_e_kernel(const SlotDesc<S> *__restrict__ descs, const WorkItem *__restrict__ work, int nwork,
                              unsigned long long *maxbits, int cur_ep) {
@@ -156,8 +161,9 @@ __global__ void max_e_kernel(const SlotDesc<S> *__restrict__ descs, const WorkIt
         double v = 0.0;
         if (i < d.nx && r < d.ny * d.nz) {
             const int j = r % d.ny, k = r / d.ny;
-            v = (double)d.ep[cur_ep][0][(i + 2) + (long long)d.ncx * (j + 2) + d.plane * (k + 2)];
-            if (!(v > 0.0)) v = 0.0;
+            const long long s = (i + 2) + (long long)d.ncx * (j + 2) + d.plane * (k + 2);
+            v = (double)d.ep[cur_ep][0][s];
+            if (!(v > 0.0) || d.fallback[s]) v = 0.0;
         }
         unsigned long long b = (unsigned long long)__double_as_longlong(v);
         for (int o = 16; o > 0; o >>= 1) {
@@ -221,26 +227,47 @@ __global__ void observables_kernel(const SlotDesc<S> *__restrict__ descs, const 
     }
 }
 
-template <typename S, int PHYS, int KIND, bool EXACT>
+template <typename S, int PHYS, int KIND, bool EXACT, int MINB>
 int blocks_per_sm() {
     static int cached = 0;
     if (!cached) {
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<S, PHYS, KIND, EXACT>, kTX * kTY, 0) !=
-                cudaSuccess || n < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<S, PHYS, KIND, EXACT, MINB>, kTX * kTY,
+                                                          0) != cudaSuccess ||
+            n < 1)
             n = 1;
         cached = n;
     }
     return cached;
 }
 
+// A persistent grid of (SMs x resident blocks) walks the work-list.
+template <typename S, int PHYS, int KIND, bool EXACT, int MINB>
+cudaError_t launch_minb(const SlotDesc<S> *descs, const SlotClock *clk, const WorkItem *work, int nwork, int stage,
+                        const Eos &eos, int sms, cudaStream_t stream) {
+    const int grid = std::min(nwork, sms * blocks_per_sm<S, PHYS, KIND, EXACT, MINB>());
+    batch_kernel<S, PHYS, KIND, EXACT, MINB><<<grid, dim3(kTX, kTY), 0, stream>>>(descs, clk, work, nwork, stage, eos);
+    return cudaGetLastError();
+}
+
+// minb: the register-cap variant (face kinds 3, 4, 5; cell kinds 2, 3, 4).
 template <typename S, int PHYS, int KIND, bool EXACT>
 cudaError_t launch_kind(const SlotDesc<S> *descs, const SlotClock *clk, const WorkItem *work, int nwork, int stage,
-                        const Eos &eos, int sms, cudaStream_t stream) {
+                        const Eos &eos, int sms, int minb, cudaStream_t stream) {
     if (nwork <= 0) return cudaSuccess;
-    const int grid = std::min(nwork, sms * blocks_per_sm<S, PHYS, KIND, EXACT>());
-    batch_kernel<S, PHYS, KIND, EXACT><<<grid, dim3(kTX, kTY), 0, stream>>>(descs, clk, work, nwork, stage, eos);
-    return cudaGetLastError();
+    constexpr bool FACE = KIND <= K_FZ;
+    switch (minb) {
+    case 2:
+        if (FACE) break;
+        return launch_minb<S, PHYS, KIND, EXACT, 2>(descs, clk, work, nwork, stage, eos, sms, stream);
+    case 3: return launch_minb<S, PHYS, KIND, EXACT, 3>(descs, clk, work, nwork, stage, eos, sms, stream);
+    case 4: return launch_minb<S, PHYS, KIND, EXACT, 4>(descs, clk, work, nwork, stage, eos, sms, stream);
+    case 5:
+        if (!FACE) break;
+        return launch_minb<S, PHYS, KIND, EXACT, 5>(descs, clk, work, nwork, stage, eos, sms, stream);
+    default: break;
+    }
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace
@@ -279,6 +306,7 @@ struct vah_batch {
     std::vector<Slot> slots;
     std::vector<unsigned char> desc_host;  // host mirror of the descriptor array
     WorkItem *d_work[vah::K_NUM];
+    int minb[vah::K_NUM];  // register-cap variant per launch kind (autotuned)
     int nwork[vah::K_NUM], cap_work[vah::K_NUM];
     double *d_partial;
     int cap_partial;
@@ -309,7 +337,8 @@ int cuda_status(cudaError_t e) {
 int nq_of(int physics) { return physics == VAH_IDEAL ? 5 : (physics == VAH_PIMUNU ? 15 : 16); }
 
 // Arrays of one event in its allocation: 16 q, 16 qS, 4 e/p, 4 uA, 4 uB,
-// 4 uS, and the face buffers (H, plus HR for reference faces) per axis.
+// 4 uS, and the face buffers (H, plus HR for reference faces) per axis; then
+// one byte per cell of fallback flags.
 int arrays_per_event(const vah_batch *b, const vah_lattice *lat) {
     const int ndir = lat->nz > 1 ? 3 : 2;
     const int per_face = b->opt.flux == VAH_FLUX_PER_CELL ? 2 : 1;
@@ -319,7 +348,7 @@ int arrays_per_event(const vah_batch *b, const vah_lattice *lat) {
 size_t event_bytes(const vah_batch *b, const vah_lattice *lat) {
     const size_t ncell = (size_t)(lat->nx + 4) * (lat->ny + 4) * (lat->nz + 4);
     const size_t per = (ncell * b->elem + 255) / 256 * 256;
-    return per * arrays_per_event(b, lat) + 256;
+    return per * arrays_per_event(b, lat) + (ncell + 255) / 256 * 256 + 256;
 }
 
 vah::Eos batch_eos(const vah_batch *b) {
@@ -376,6 +405,7 @@ int fill_slot(vah_batch *b, int slot) {
             d.H[k][n] = next();
             if (b->opt.flux == VAH_FLUX_PER_CELL) d.HR[k][n] = next();
         }
+    d.fallback = (unsigned char *)(base + off);
     *desc_host<S>(b, slot) = d;
     VAH_TRY(cudaMemcpyAsync((char *)b->d_desc + sizeof(SlotDesc<S>) * slot, &d, sizeof(d), cudaMemcpyHostToDevice,
                             b->stream));
@@ -421,18 +451,29 @@ int rebuild_work(vah_batch *b) {
     return VAH_OK;
 }
 
+// One launch of a kind known at run time, with the batch's register-cap choice.
+template <typename S, int PHYS, bool EXACT>
+cudaError_t launch_kind_rt(vah_batch *b, const SlotDesc<S> *descs, int kind, int stage, const vah::Eos &eos) {
+    using namespace vah;
+    const WorkItem *w = b->d_work[kind];
+    const int n = b->nwork[kind], m = b->minb[kind];
+    switch (kind) {
+    case K_FX: return launch_kind<S, PHYS, K_FX, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
+    case K_FY: return launch_kind<S, PHYS, K_FY, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
+    case K_FZ: return launch_kind<S, PHYS, K_FZ, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
+    case K_C2: return launch_kind<S, PHYS, K_C2, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
+    case K_C3: return launch_kind<S, PHYS, K_C3, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 template <typename S, int PHYS, bool EXACT>
 int enqueue_step(vah_batch *b) {
     using namespace vah;
     const SlotDesc<S> *descs = (const SlotDesc<S> *)b->d_desc;
     const Eos eos = batch_eos(b);
-    for (int stage = 1; stage <= 2; ++stage) {
-        VAH_TRY((launch_kind<S, PHYS, K_FX, EXACT>(descs, b->d_clk, b->d_work[K_FX], b->nwork[K_FX], stage, eos, b->sms, b->stream)));
-        VAH_TRY((launch_kind<S, PHYS, K_FY, EXACT>(descs, b->d_clk, b->d_work[K_FY], b->nwork[K_FY], stage, eos, b->sms, b->stream)));
-        VAH_TRY((launch_kind<S, PHYS, K_FZ, EXACT>(descs, b->d_clk, b->d_work[K_FZ], b->nwork[K_FZ], stage, eos, b->sms, b->stream)));
-        VAH_TRY((launch_kind<S, PHYS, K_C2, EXACT>(descs, b->d_clk, b->d_work[K_C2], b->nwork[K_C2], stage, eos, b->sms, b->stream)));
-        VAH_TRY((launch_kind<S, PHYS, K_C3, EXACT>(descs, b->d_clk, b->d_work[K_C3], b->nwork[K_C3], stage, eos, b->sms, b->stream)));
-    }
+    for (int stage = 1; stage <= 2; ++stage)
+        for (int kind = 0; kind < K_NUM; ++kind) VAH_TRY((launch_kind_rt<S, PHYS, EXACT>(b, descs, kind, stage, eos)));
     advance_kernel<<<(kMaxSlots + 255) / 256, 256, 0, b->stream>>>(b->d_clk, b->d_dt, kMaxSlots);
     VAH_TRY(cudaGetLastError());
     return VAH_OK;
@@ -546,6 +587,7 @@ extern "C" int vah_batch_create(const vah_options *opt, const double *eos_table,
     b->own_stream = opt->stream == nullptr;
     b->capacity = capacity_bytes;
     b->used = 0;
+    for (int k = 0; k < vah::K_NUM; ++k) b->minb[k] = k <= vah::K_FZ ? 4 : 3;  // untuned default
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, opt->device);
     int rc = VAH_OK;
     auto chk = [&](cudaError_t e) {
@@ -851,4 +893,90 @@ extern "C" int vah_batch_kernel_time(vah_batch *b, double *ms, long long *steps)
     b->kernel_ms = 0;
     b->kernel_steps = 0;
     return VAH_OK;
+}
+
+namespace {
+
+// The batch form of vah_event_autotune: every register-cap variant of each
+// launch kind runs over the whole work-list in stage-1 buffer roles (outputs
+// are stage scratch), the fastest is kept, the per-slot counters are restored
+// and the step graph is re-captured at the next step.
+template <typename S, int PHYS, bool EXACT>
+int batch_autotune_t(vah_batch *b, int reps, vah_tune_report *out) {
+    using namespace vah;
+    const SlotDesc<S> *descs = (const SlotDesc<S> *)b->d_desc;
+    const Eos eos = batch_eos(b);
+    std::vector<unsigned long long> saved((size_t)kMaxSlots * 4);
+    VAH_TRY(cudaStreamSynchronize(b->stream));
+    VAH_TRY(cudaMemcpy(saved.data(), b->d_counters, saved.size() * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost));
+    cudaEvent_t e0, e1;
+    VAH_TRY(cudaEventCreate(&e0));
+    VAH_TRY(cudaEventCreate(&e1));
+    int rc = VAH_OK;
+    out->nkinds = K_NUM;
+    for (int kind = 0; kind < K_NUM && rc == VAH_OK; ++kind) {
+        vah_launch_choice &r = out->kind[kind];
+        const int def = b->minb[kind];
+        r = {kTX, kTY, def, 0.0, 0.0};
+        if (b->nwork[kind] == 0) continue;
+        const int *cand = kind <= K_FZ ? kFaceMinb : kCellMinb;
+        double best = 1e300;
+        int pick = def;
+        for (int c = 0; c < kNumMinb && rc == VAH_OK; ++c) {
+            b->minb[kind] = cand[c];
+            auto launch = [&]() { return launch_kind_rt<S, PHYS, EXACT>(b, descs, kind, 1, eos); };
+            if (launch() != cudaSuccess || cudaEventRecord(e0, b->stream) != cudaSuccess) {
+                rc = VAH_ERR_CUDA;
+                break;
+            }
+            for (int k = 0; k < reps && rc == VAH_OK; ++k)
+                if (launch() != cudaSuccess) rc = VAH_ERR_CUDA;
+            float f = 0;
+            if (rc != VAH_OK || cudaEventRecord(e1, b->stream) != cudaSuccess ||
+                cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&f, e0, e1) != cudaSuccess) {
+                rc = VAH_ERR_CUDA;
+                break;
+            }
+            const double ms = f / reps;
+            if (cand[c] == def) r.ms_default = ms;
+            if (ms < best) {
+                best = ms;
+                pick = cand[c];
+            }
+        }
+        b->minb[kind] = pick;
+        r = {kTX, kTY, pick, r.ms_default, best};
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cudaMemcpy(b->d_counters, saved.data(), saved.size() * sizeof(unsigned long long),
+                   cudaMemcpyHostToDevice) != cudaSuccess &&
+        rc == VAH_OK)
+        rc = VAH_ERR_CUDA;
+    b->dirty = true;  // the step graph holds the old choice
+    return rc;
+}
+
+template <typename S>
+int batch_autotune_s(vah_batch *b, int reps, vah_tune_report *out) {
+    const bool exact = b->opt.flux == VAH_FLUX_PER_CELL;
+    switch (b->opt.physics) {
+    case VAH_IDEAL: return exact ? batch_autotune_t<S, 0, true>(b, reps, out) : batch_autotune_t<S, 0, false>(b, reps, out);
+    case VAH_PIMUNU: return exact ? batch_autotune_t<S, 1, true>(b, reps, out) : batch_autotune_t<S, 1, false>(b, reps, out);
+    default: return exact ? batch_autotune_t<S, 2, true>(b, reps, out) : batch_autotune_t<S, 2, false>(b, reps, out);
+    }
+}
+
+}  // namespace
+
+extern "C" int vah_batch_autotune(vah_batch *b, int reps, vah_tune_report *out) {
+    if (!b || !out || reps < 1) return VAH_ERR_ARG;
+    memset(out, 0, sizeof(*out));
+    VAH_TRY(cudaSetDevice(b->opt.device));
+    if (b->dirty) {  // the work-list must describe the admitted events
+        const int rc = rebuild_work(b);
+        if (rc != VAH_OK) return rc;
+    }
+    return b->elem == sizeof(float) ? batch_autotune_s<float>(b, reps, out) : batch_autotune_s<double>(b, reps, out);
 }

@@ -1,17 +1,26 @@
-// vah_kernels.cu -- CUDA kernels of the VAH time step (sm_100a).
+// vah_kernels_impl.cuh -- CUDA kernels of the VAH time step (sm_100a) and
+// their launch dispatch. Compiled once per storage type by vah_kernels_f64.cu
+// and vah_kernels_f32.cu (separate translation units build in parallel).
 //
 // stage_kernel: one thread per interior cell runs the whole RK stage of that
-// cell (vah_stage.cuh). The step is FP64-arithmetic-bound (13 Newton
-// inversions per cell and stage in the reference-faithful flux mode), so the
-// launch favours occupancy: 128-thread blocks shaped 32 (x) by 4 (y*z rows),
-// x fastest so that every load of a field is a coalesced 32-wide row.
+// cell (vah_stage.cuh). face_kernel + cell_kernel: the same stage split into
+// per-axis face launches and one cell launch (the default path).
+// The step is FP64-arithmetic-bound (13 Newton inversions per cell and stage
+// in the reference-faithful flux mode), so launches favour occupancy:
+// 128-thread blocks, x fastest so that every load of a field is a coalesced
+// row. The split kernels come in register-cap variants (MINB = the minimum
+// number of resident 128-thread blocks per SM the compiler must allow) and
+// take their block shape at run time; the autotuner picks both per launch
+// kind by timing them on the event's own state.
+#pragma once
+
 #include "vah_kernels.cuh"
 
 namespace vah {
 
 namespace {
 
-constexpr int kBX = 32, kBY = 4;
+constexpr int kBX = 32, kBY = 4;  // fused stage kernel shape
 
 template <typename S, int PHYS, bool IS3D>
 __global__ void __launch_bounds__(kBX *kBY) stage_kernel(const StageArgs<S> a) {
@@ -24,13 +33,13 @@ __global__ void __launch_bounds__(kBX *kBY) stage_kernel(const StageArgs<S> a) {
 
 // Faces at +1/2 of the ghosted cells along DIR that bound an interior cell:
 // left cell index 1 .. n along DIR (ghost layer 1 included), interior across.
-template <typename S, int PHYS, int DIR, bool EXACT>
-__global__ void __launch_bounds__(kBX *kBY) face_kernel(const StageArgs<S> a) {
+template <typename S, int PHYS, int DIR, bool EXACT, int MINB>
+__global__ void __launch_bounds__(kSplitThreads, MINB) face_kernel(const StageArgs<S> a) {
     const int ext0 = DIR == 0 ? a.nx + 1 : a.nx;
     const int ext1 = DIR == 1 ? a.ny + 1 : a.ny;
     const int ext2 = DIR == 2 ? a.nz + 1 : a.nz;
-    const int i = blockIdx.x * kBX + threadIdx.x;
-    const int r = blockIdx.y * kBY + threadIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= ext0 || r >= ext1 * ext2) return;
     const int j = r % ext1, k = r / ext1;
     const int gi = i + (DIR == 0 ? 1 : 2), gj = j + (DIR == 1 ? 1 : 2), gk = k + (DIR == 2 ? 1 : 2);
@@ -43,10 +52,10 @@ __global__ void __launch_bounds__(kBX *kBY) face_kernel(const StageArgs<S> a) {
     }
 }
 
-template <typename S, int PHYS, bool IS3D, bool EXACT>
-__global__ void __launch_bounds__(kBX *kBY) cell_kernel(const StageArgs<S> a) {
-    const int i = blockIdx.x * kBX + threadIdx.x;
-    const int r = blockIdx.y * kBY + threadIdx.y;
+template <typename S, int PHYS, bool IS3D, bool EXACT, int MINB>
+__global__ void __launch_bounds__(kSplitThreads, MINB) cell_kernel(const StageArgs<S> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= a.nx || r >= a.ny * a.nz) return;
     const int j = r % a.ny, k = r / a.ny;
     cell_compute<S, PHYS, IS3D, EXACT>(a, i + 2, j + 2, k + 2);
@@ -124,20 +133,43 @@ cudaError_t stage_dispatch(const StageArgs<S> &a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-template <typename S, int PHYS, bool EXACT>
-cudaError_t split_dispatch(const StageArgs<S> &a, cudaStream_t stream) {
-    dim3 block(kBX, kBY);
-    face_kernel<S, PHYS, 0, EXACT><<<dim3((a.nx + 1 + kBX - 1) / kBX, (a.ny * a.nz + kBY - 1) / kBY), block, 0, stream>>>(a);
-    face_kernel<S, PHYS, 1, EXACT><<<dim3((a.nx + kBX - 1) / kBX, ((a.ny + 1) * a.nz + kBY - 1) / kBY), block, 0, stream>>>(a);
-    if (a.nz > 1)
-        face_kernel<S, PHYS, 2, EXACT>
-            <<<dim3((a.nx + kBX - 1) / kBX, (a.ny * (a.nz + 1) + kBY - 1) / kBY), block, 0, stream>>>(a);
-    dim3 grid((a.nx + kBX - 1) / kBX, (a.ny * a.nz + kBY - 1) / kBY);
-    if (a.nz > 1)
-        cell_kernel<S, PHYS, true, EXACT><<<grid, block, 0, stream>>>(a);
-    else
-        cell_kernel<S, PHYS, false, EXACT><<<grid, block, 0, stream>>>(a);
+// One launch of a split kernel kind with the given shape and register-cap variant.
+template <typename S, int PHYS, bool EXACT, int DIR>
+cudaError_t face_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t stream) {
+    const int ext0 = DIR == 0 ? a.nx + 1 : a.nx;
+    const int rows = (DIR == 1 ? a.ny + 1 : a.ny) * (DIR == 2 ? a.nz + 1 : a.nz);
+    const dim3 block(c.bx, c.by), grid((ext0 + c.bx - 1) / c.bx, (rows + c.by - 1) / c.by);
+    switch (c.minb) {
+    case 3: face_kernel<S, PHYS, DIR, EXACT, 3><<<grid, block, 0, stream>>>(a); break;
+    case 4: face_kernel<S, PHYS, DIR, EXACT, 4><<<grid, block, 0, stream>>>(a); break;
+    case 5: face_kernel<S, PHYS, DIR, EXACT, 5><<<grid, block, 0, stream>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
+}
+
+template <typename S, int PHYS, bool EXACT, bool IS3D>
+cudaError_t cell_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t stream) {
+    const dim3 block(c.bx, c.by), grid((a.nx + c.bx - 1) / c.bx, (a.ny * a.nz + c.by - 1) / c.by);
+    switch (c.minb) {
+    case 2: cell_kernel<S, PHYS, IS3D, EXACT, 2><<<grid, block, 0, stream>>>(a); break;
+    case 3: cell_kernel<S, PHYS, IS3D, EXACT, 3><<<grid, block, 0, stream>>>(a); break;
+    case 4: cell_kernel<S, PHYS, IS3D, EXACT, 4><<<grid, block, 0, stream>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename S, int PHYS, bool EXACT>
+cudaError_t split_kind_dispatch(const StageArgs<S> &a, int kind, const KindConfig &c, cudaStream_t stream) {
+    switch (kind) {
+    case kFaceX: return face_launch<S, PHYS, EXACT, 0>(a, c, stream);
+    case kFaceY: return face_launch<S, PHYS, EXACT, 1>(a, c, stream);
+    case kFaceZ: return a.nz > 1 ? face_launch<S, PHYS, EXACT, 2>(a, c, stream) : cudaSuccess;
+    case kCell:
+        return a.nz > 1 ? cell_launch<S, PHYS, EXACT, true>(a, c, stream) : cell_launch<S, PHYS, EXACT, false>(a, c, stream);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 int grid_for(long long n, int block) {
@@ -160,14 +192,36 @@ cudaError_t launch_stage(const StageArgs<S> &a, int physics, cudaStream_t stream
 }
 
 template <typename S>
-cudaError_t launch_stage_split(const StageArgs<S> &a, int physics, bool exact, cudaStream_t stream) {
+cudaError_t launch_split_kind(const StageArgs<S> &a, int physics, bool exact, int kind, const KindConfig &c,
+                              cudaStream_t stream) {
+    if (!valid_kind_config(kind, c)) return cudaErrorInvalidValue;
     switch (physics) {
-    case kIdeal: return exact ? split_dispatch<S, kIdeal, true>(a, stream) : split_dispatch<S, kIdeal, false>(a, stream);
-    case kPimunu: return exact ? split_dispatch<S, kPimunu, true>(a, stream) : split_dispatch<S, kPimunu, false>(a, stream);
+    case kIdeal:
+        return exact ? split_kind_dispatch<S, kIdeal, true>(a, kind, c, stream)
+                     : split_kind_dispatch<S, kIdeal, false>(a, kind, c, stream);
+    case kPimunu:
+        return exact ? split_kind_dispatch<S, kPimunu, true>(a, kind, c, stream)
+                     : split_kind_dispatch<S, kPimunu, false>(a, kind, c, stream);
     case kPimunuPi:
-        return exact ? split_dispatch<S, kPimunuPi, true>(a, stream) : split_dispatch<S, kPimunuPi, false>(a, stream);
+        return exact ? split_kind_dispatch<S, kPimunuPi, true>(a, kind, c, stream)
+                     : split_kind_dispatch<S, kPimunuPi, false>(a, kind, c, stream);
     default: return cudaErrorInvalidValue;
     }
+}
+
+template <typename S>
+cudaError_t launch_stage_split(const StageArgs<S> &a, int physics, bool exact, const SplitConfig &c,
+                               cudaStream_t stream) {
+    for (int kind = 0; kind < kNumSplitKinds; ++kind) {
+        const cudaError_t e = launch_split_kind<S>(a, physics, exact, kind, c.k[kind], stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <typename S>
+cudaError_t launch_stage_split(const StageArgs<S> &a, int physics, bool exact, cudaStream_t stream) {
+    return launch_stage_split<S>(a, physics, exact, default_split_config(), stream);
 }
 
 template <typename S>
@@ -212,13 +266,15 @@ cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cud
 
 #define VAH_INSTANTIATE(S)                                                                                      \
     template cudaError_t launch_stage<S>(const StageArgs<S> &, int, cudaStream_t);                              \
+    template cudaError_t launch_split_kind<S>(const StageArgs<S> &, int, bool, int, const KindConfig &,         \
+                                              cudaStream_t);                                                    \
+    template cudaError_t launch_stage_split<S>(const StageArgs<S> &, int, bool, const SplitConfig &,            \
+                                               cudaStream_t);                                                   \
     template cudaError_t launch_stage_split<S>(const StageArgs<S> &, int, bool, cudaStream_t);                  \
     template cudaError_t launch_set_conserved<S>(const FieldSet<S> &, const FieldSet<S> &, const FieldSet<S> &, \
                                                  const S *, int, int, int, int, double, int, cudaStream_t);     \
     template cudaError_t launch_init_primitives<S>(const FieldSet<S> &, const FieldSet<S> &, const S *, S *,    \
                                                    const Eos &, int, int, int, cudaStream_t);                  \
     template cudaError_t launch_ghosts<S>(const FieldSet<S> &, int, int, int, cudaStream_t);
-VAH_INSTANTIATE(double)
-VAH_INSTANTIATE(float)
 
 }  // namespace vah

@@ -61,7 +61,8 @@ double energy_at_temperature(const std::vector<double> &tab, int eos, double T) 
 
 extern "C" int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res, double *latencies,
                              int max_latencies) {
-    if (!cfg || !res || cfg->rate <= 0 || cfg->duration_s <= 0 || cfg->chunk_steps < 1) return VAH_ERR_ARG;
+    if (!cfg || !res || cfg->rate <= 0 || cfg->duration_s <= 0 || cfg->chunk_steps < 1 || !(cfg->e_floor >= 0))
+        return VAH_ERR_ARG;
     std::vector<double> tab;
     if (cfg->eos == VAH_EOS_TABLE) {
         tab.assign(VAH_EOS_TABLE_LEN(VAH_EOS_TABLE_N), 0.0);
@@ -116,10 +117,11 @@ extern "C" int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res,
             if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
             std::vector<double> exy((size_t)r.lat.nx * r.lat.ny), f(r.lat.nz), e((size_t)r.lat.nx * r.lat.ny * r.lat.nz);
             vah_ic_mc_glauber(r.lat.nx, r.lat.ny, r.lat.dx, r.lat.dy, r.b, 4.2, 197, 6.38, 0.535, 0.5, r.seed, e_peak,
-                              1e-3, exy.data(), nullptr);
+                              0.0, exy.data(), nullptr);
             vah_ic_longitudinal(r.lat.nz, r.lat.dz, 1.5, 1.3, f.data());
+            // the floor goes on after the product, as InitialConditions.cpp:247 adds it
             for (int k2 = 0; k2 < r.lat.nz; ++k2)
-                for (size_t s = 0; s < exy.size(); ++s) e[s + exy.size() * k2] = exy[s] * f[k2];
+                for (size_t s = 0; s < exy.size(); ++s) e[s + exy.size() * k2] = exy[s] * f[k2] + cfg->e_floor;
             std::lock_guard<std::mutex> lock(mu);
             r.e = std::move(e);
             r.ready = true;
@@ -137,8 +139,8 @@ extern "C" int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res,
     std::vector<double> lat_s;
     std::vector<int> queue_order;  // arrived requests, arrival order
     int next_admit = 0;            // requests admitted or refused so far, in arrival order
-    long long cell_updates = 0, chunk_count = 0, max_resident = 0, timeouts = 0, rejected = 0;
-    double last_done = 0;
+    long long cell_updates = 0, chunk_count = 0, max_resident = 0, timeouts = 0, rejected = 0, failed = 0;
+    double last_done = 0, tau_freeze_max = 0;
     std::vector<double> emax;
     rc = VAH_OK;
     while (rc == VAH_OK) {
@@ -193,13 +195,18 @@ extern "C" int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res,
         for (const Live &l : live) {
             vah_event_info info;
             vah_batch_event_info(batch, l.slot, &info);
-            const bool frozen = emax[l.slot] < e_freeze;
+            const bool frozen = info.nan_cells == 0 && emax[l.slot] < e_freeze;
             const bool too_old = info.t > cfg->t_max;
             if (frozen || too_old || info.nan_cells > 0) {
                 const double now = seconds_since(t_start);
-                lat_s.push_back(now - reqs[l.req].arrival);
-                last_done = now;
-                if (!frozen) ++timeouts;
+                if (frozen) {  // latency statistics cover events that reached freeze-out
+                    lat_s.push_back(now - reqs[l.req].arrival);
+                    last_done = now;
+                    tau_freeze_max = std::max(tau_freeze_max, info.t);
+                } else {
+                    ++timeouts;
+                    if (info.nan_cells > 0) ++failed;
+                }
                 vah_batch_remove(batch, l.slot);
             } else {
                 keep.push_back(l);
@@ -231,6 +238,8 @@ extern "C" int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res,
     res->cell_updates_per_s = res->wall_s > 0 ? cell_updates / res->wall_s : 0.0;
     res->max_resident = max_resident;
     res->chunks = chunk_count;
+    res->failed = failed;
+    res->tau_freeze_max = tau_freeze_max;
     if (latencies)
         for (int k = 0; k < max_latencies && k < (int)lat_s.size(); ++k) latencies[k] = lat_s[k];
     return VAH_OK;

@@ -37,6 +37,7 @@ struct StageArgs {
     S *eout, *pout;
     Eos eos;
     unsigned long long *counters;  // [face fallbacks, cell fallbacks, NaN cells]
+    unsigned char *fallback;       // optional: per ghosted cell, 1 where this stage's inversion fell back
     // face/cell split: flux through the face at +1/2 of ghosted cell s along
     // axis d, field n, as cell s evaluates it (H) and as cell s+1 does (HR,
     // reference face semantics only); scratch of ncell entries per field
@@ -185,6 +186,7 @@ VAH_HD void stage_cell(const StageArgs<S> &a, int i, int j, int k) {
     if ((fails & 255u) && a.counters) count_add(a.counters + 0, fails & 255u);
     if (st != 0 && a.counters) count_add(a.counters + 1, 1ull);
     if ((bad || st == 2 || (fails >> 8)) && a.counters) count_add(a.counters + 2, 1ull);
+    if (a.fallback) a.fallback[s] = st != 0;
 
     store_cell(a, s, NQ, val, u, e, p);
     // face ghost layers (setGhostCellsKernelI/J/K, DynamicalVariables.cpp:400-489)
@@ -285,6 +287,7 @@ VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
     regulate<PHYS>(a.t_inv, e, p, val, u);
     if (st != 0 && a.counters) count_add(a.counters + 1, 1ull);
     if ((bad || st == 2) && a.counters) count_add(a.counters + 2, 1ull);
+    if (a.fallback) a.fallback[s] = st != 0;
     store_cell(a, s, NQ, val, u, e, p);
     const long long sy = a.ncx, sz = a.plane;
     if (i == 2) { store_cell(a, s - 1, NQ, val, u, e, p); store_cell(a, s - 2, NQ, val, u, e, p); }

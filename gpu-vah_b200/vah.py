@@ -52,6 +52,19 @@ class Options(C.Structure):
                 ("stream", C.c_void_p)]
 
 
+class LaunchChoice(C.Structure):
+    _fields_ = [("bx", C.c_int), ("by", C.c_int), ("minb", C.c_int), ("ms_default", C.c_double),
+                ("ms_best", C.c_double)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("nkinds", C.c_int), ("kind", LaunchChoice * 5)]
+
+    def as_list(self):
+        return [{"block": [k.bx, k.by], "minb": k.minb, "ms_default": k.ms_default, "ms_best": k.ms_best}
+                for k in self.kind[:self.nkinds]]
+
+
 class Stats(C.Structure):
     _fields_ = [("face_fallbacks", C.c_longlong), ("cell_fallbacks", C.c_longlong), ("nan_cells", C.c_longlong),
                 ("steps", C.c_longlong)]
@@ -61,7 +74,7 @@ EXPORTS = ["vah_version", "vah_eos_table_build", "vah_event_create", "vah_event_
            "vah_event_get_field", "vah_event_set_conserved", "vah_event_init_from_e", "vah_event_set_ghost_cells",
            "vah_rk2_step", "vah_run", "vah_event_sync", "vah_event_stats", "vah_event_set_timing",
            "vah_event_kernel_time", "vah_rk2_step_host", "vah_ic_optical_glauber", "vah_ic_mc_glauber",
-           "vah_ic_longitudinal"]
+           "vah_ic_longitudinal", "vah_event_autotune", "vah_batch_autotune"]
 
 _lib = None
 
@@ -85,6 +98,7 @@ def library():
         for name in ("vah_event_destroy", "vah_event_set_ghost_cells", "vah_event_sync"):
             getattr(L, name).argtypes = [C.c_void_p]
         L.vah_event_set_field.argtypes = [C.c_void_p, I, P, I]
+        L.vah_event_autotune.argtypes = [C.c_void_p, I, C.POINTER(TuneReport)]
         L.vah_event_get_field.argtypes = [C.c_void_p, I, P, I]
         L.vah_event_set_conserved.argtypes = [C.c_void_p, D, I]
         L.vah_event_init_from_e.argtypes = [C.c_void_p, D, P, I]
@@ -214,6 +228,12 @@ class Event:
         check(self.L.vah_event_kernel_time(self.ev, C.byref(ms), C.byref(n)), "vah_event_kernel_time")
         return ms.value, n.value
 
+    def autotune(self, reps=3):
+        """Pick the fastest launch configuration per kernel kind (vah_event_autotune); returns the choices."""
+        r = TuneReport()
+        check(self.L.vah_event_autotune(self.ev, int(reps), C.byref(r)), "vah_event_autotune")
+        return r.as_list()
+
     def step_host(self, t, dt, ptrs):
         """Host-buffer step: ptrs = list of NUM_FIELDS host addresses (0 for unused)."""
         arr = (P * NUM_FIELDS)(*[C.cast(C.c_void_p(p), P) if p else P() for p in ptrs])
@@ -232,6 +252,7 @@ def _batch_lib():
     L = library()
     if not getattr(L, "_batch_ready", False):
         L.vah_batch_create.argtypes = [C.POINTER(Options), P, C.c_size_t, C.POINTER(C.c_void_p)]
+        L.vah_batch_autotune.argtypes = [C.c_void_p, I, C.POINTER(TuneReport)]
         for name in ("vah_batch_destroy", "vah_batch_sync"):
             getattr(L, name).argtypes = [C.c_void_p]
         L.vah_batch_event_bytes.argtypes = [C.c_void_p, C.POINTER(Lattice), C.POINTER(C.c_size_t)]
@@ -331,31 +352,41 @@ class Batch:
         check(self.L.vah_batch_kernel_time(self.b, C.byref(ms), C.byref(n)), "vah_batch_kernel_time")
         return ms.value, n.value
 
+    def autotune(self, reps=3):
+        """Pick the fastest register-cap variant per launch kind (vah_batch_autotune); returns the choices."""
+        r = TuneReport()
+        check(self.L.vah_batch_autotune(self.b, int(reps), C.byref(r)), "vah_batch_autotune")
+        return r.as_list()
+
 
 class ServeConfig(C.Structure):
     _fields_ = [("rate", D), ("duration_s", D), ("seed", C.c_ulonglong), ("frac_3d", D), ("side2_min", I),
                 ("side2_max", I), ("side3_min", I), ("side3_max", I), ("nz3_min", I), ("nz3_max", I), ("dx", D),
                 ("deta", D), ("b_max", D), ("t0", D), ("dt", D), ("eta_over_s", D), ("T0_GeV", D), ("Tf_GeV", D),
                 ("t_max", D), ("physics", I), ("eos", I), ("precision", I), ("flux", I), ("device", I),
-                ("capacity_bytes", C.c_size_t), ("chunk_steps", I), ("ic_threads", I)]
+                ("capacity_bytes", C.c_size_t), ("chunk_steps", I), ("ic_threads", I), ("e_floor", D)]
 
 
 class ServeResult(C.Structure):
     _fields_ = [("offered", C.c_longlong), ("completed", C.c_longlong), ("timeouts", C.c_longlong),
                 ("rejected", C.c_longlong), ("wall_s", D), ("events_per_s", D), ("p50_s", D), ("p99_s", D),
                 ("cell_updates", C.c_longlong), ("cell_updates_per_s", D), ("max_resident", C.c_longlong),
-                ("chunks", C.c_longlong)]
+                ("chunks", C.c_longlong), ("failed", C.c_longlong), ("tau_freeze_max", D)]
 
 
 def serve(**kw):
-    """Run the continuous-batching request loop (vah_serve_run); returns (result dict, latencies)."""
+    """Run the continuous-batching request loop (vah_serve_run); returns (result dict, latencies).
+
+    Defaults: peak temperature 0.4 GeV and an initial floor of 0.01 fm^-4. At a 0.6 GeV peak with the
+    reference's 1e-3 floor, lumpy 0.2 fm grids drive most dilute cells into the inversion fallback and
+    leave isolated single-cell spikes far above their neighbours, which keep max T above freeze-out."""
     L = library()
     L.vah_serve_run.argtypes = [C.POINTER(ServeConfig), C.POINTER(ServeResult), P, I]
     cfg = dict(rate=50.0, duration_s=10.0, seed=1, frac_3d=0.3, side2_min=61, side2_max=261, side3_min=81,
                side3_max=161, nz3_min=41, nz3_max=81, dx=0.2, deta=0.2, b_max=14.0, t0=0.25, dt=0.02,
-               eta_over_s=0.16, T0_GeV=0.6, Tf_GeV=0.150, t_max=40.0, physics=VAH_PIMUNU_PI, eos=VAH_EOS_TABLE,
+               eta_over_s=0.16, T0_GeV=0.4, Tf_GeV=0.150, t_max=100.0, physics=VAH_PIMUNU_PI, eos=VAH_EOS_TABLE,
                precision=VAH_FP64, flux=VAH_FLUX_PER_CELL, device=0, capacity_bytes=120 << 30, chunk_steps=10,
-               ic_threads=16)
+               ic_threads=16, e_floor=1e-2)
     cfg.update(kw)
     c = ServeConfig(**cfg)
     r = ServeResult()

@@ -189,6 +189,27 @@ int vah_event_stats(vah_event *ev, vah_stats *out);
 int vah_event_set_timing(vah_event *ev, int on);
 int vah_event_kernel_time(vah_event *ev, double *ms, long long *launches);
 
+/* ---- launch autotuning (no reference counterpart) ----
+ * The face/cell kernels come in register-cap variants and take their block
+ * shape at run time. vah_event_autotune times every candidate of each launch
+ * kind (face x, face y, face z, cell; `reps` timed launches each, after one
+ * warm-up) on the event's current state, keeps the fastest for the event's
+ * later steps, and reports the choice and its time next to the default's.
+ * It writes only stage scratch (the state is unchanged) and synchronises the
+ * event's stream. Results do not depend on the choice. The fused flux mode has
+ * nothing to tune (nkinds = 0). vah_batch_autotune does the same for a
+ * batch's persistent launches (register cap only; tiles stay 32 x 4). */
+typedef struct vah_launch_choice {
+    int bx, by, minb;   /* block shape and minimum resident blocks per SM the compiler was held to */
+    double ms_default;  /* ms per launch of the configuration in use before the call */
+    double ms_best;     /* ms per launch of the chosen configuration */
+} vah_launch_choice;
+typedef struct vah_tune_report {
+    int nkinds;
+    vah_launch_choice kind[5];
+} vah_tune_report;
+int vah_event_autotune(vah_event *ev, int reps, vah_tune_report *out);
+
 /* Host-buffer form of the reference CPU step: the caller's host arrays (the
  * reference's process globals q, e, p, u, up; fields ordered by VAH_F_*,
  * full ghosted layout) are copied in, stepped once on the GPU, and copied
@@ -233,8 +254,10 @@ int vah_batch_step(vah_batch *b, int nsteps);
 int vah_batch_sync(vah_batch *b);
 int vah_batch_event_info(vah_batch *b, int slot, vah_event_info *out);
 int vah_batch_get_field(vah_batch *b, int slot, int field, double *host, int with_ghosts);
-/* Per-slot maximum energy density over the interior (the freeze-out test:
- * max T < T_f with T monotone in e); out[s] = 0 for free slots. FP64,
+/* Per-slot maximum energy density over the interior cells whose latest
+ * inversion converged (the freeze-out test: max T < T_f with T monotone in
+ * e; a cell in the reference's inversion fallback holds e = 0.999 e_prev,
+ * not a solution, and is left out); out[s] = 0 for free slots. FP64,
  * deterministic. */
 int vah_batch_max_energy_density(vah_batch *b, double *out, int nslots);
 /* Per-slot observables in FP64 with a fixed summation order (an event's
@@ -245,6 +268,9 @@ int vah_batch_max_energy_density(vah_batch *b, double *out, int nslots);
 int vah_batch_observables(vah_batch *b, double *out, int nslots);
 int vah_batch_set_timing(vah_batch *b, int on);
 int vah_batch_kernel_time(vah_batch *b, double *ms, long long *steps);
+/* Register-cap autotuning of the batch's launch kinds (face x, y, z, cell
+ * 2+1D, cell 3+1D), as vah_event_autotune describes. */
+int vah_batch_autotune(vah_batch *b, int reps, vah_tune_report *out);
 
 /* ---- serving: continuous batching of an open-loop request stream ----
  * No reference counterpart (the reference runs one event per process). A
@@ -257,8 +283,8 @@ int vah_batch_kernel_time(vah_batch *b, double *ms, long long *steps);
  * has room (capacity_bytes), all resident events advance together in chunks
  * of chunk_steps graph-replayed steps, and an event retires when its maximum
  * temperature falls below Tf_GeV (FP64 device reduction after each chunk) or
- * its time passes t_max (counted in timeouts). Latency = arrival to
- * retirement, wall clock. latencies (optional) receives up to max_latencies
+ * its time passes t_max (counted in timeouts, not in the latency
+ * statistics). Latency = arrival to retirement at freeze-out, wall clock. latencies (optional) receives up to max_latencies
  * values in completion order. */
 typedef struct vah_serve_config {
     double rate, duration_s;
@@ -270,6 +296,7 @@ typedef struct vah_serve_config {
     int physics, eos, precision, flux, device;
     size_t capacity_bytes;
     int chunk_steps, ic_threads;
+    double e_floor;  /* energy density added to every initial cell, fm^-4 (the reference adds 1e-3) */
 } vah_serve_config;
 
 typedef struct vah_serve_result {
@@ -278,6 +305,8 @@ typedef struct vah_serve_result {
     long long cell_updates;
     double cell_updates_per_s;
     long long max_resident, chunks;
+    long long failed;       /* events retired because a NaN reached e or u (also in timeouts) */
+    double tau_freeze_max;  /* largest event time at freeze-out, fm/c */
 } vah_serve_result;
 
 int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res, double *latencies, int max_latencies);

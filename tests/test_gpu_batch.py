@@ -109,7 +109,9 @@ def test_batch_reductions_match_host():
     obs = batch.observables(n)
     for slot, (nx, ny, nz, dx, dz, b, seed, dt) in zip(slots, EVENTS):
         get = lambda f: batch.get_field(slot, f, False)
-        assert emax[slot] == np.max(get(16))
+        # cells in the inversion fallback (u = (1,0,0,0) exactly) are left out of the maximum
+        fell = (get(18) == 1.0) & (get(19) == 0.0) & (get(20) == 0.0) & (get(21) == 0.0)
+        assert emax[slot] == np.max(np.where(fell, 0.0, get(16)))
         host = OBS.observables(get, 0.4 + 5 * dt, dx, dx, dz, 2)
         assert abs(obs[slot, 0] / host["E_tot"] - 1) < 1e-12
         assert abs(obs[slot, 1] - host["eps_p"]) < 1e-12 * max(1, abs(host["eps_p"]))

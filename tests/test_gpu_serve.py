@@ -17,6 +17,7 @@ def test_serve_small_stream_completes_every_request(precision):
                                capacity_bytes=4 << 30, chunk_steps=5, ic_threads=4)
     assert res["offered"] > 10
     assert res["completed"] == res["offered"] and res["timeouts"] == 0 and res["rejected"] == 0
+    assert res["failed"] == 0 and 0 < res["tau_freeze_max"] < 30.0
     assert np.all(lat > 0) and res["p99_s"] >= res["p50_s"] > 0
     assert res["max_resident"] > 1  # requests overlapped on the device
     assert res["events_per_s"] > 0 and res["cell_updates"] > 0
