@@ -225,15 +225,25 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def traffic_per_launch(cells):
-    """DRAM bytes of one stage-kernel launch from the committed ncu summary
-    (bytes per interior cell, scaled to this launch), or None."""
-    path = os.path.join(ROOT, "profiles", "stage_kernel_dram.json")
+def traffic_per_launch(cells, flux, precision):
+    """DRAM bytes of one RK stage (its launches) from the committed ncu
+    summaries (bytes per interior cell, scaled to this event), or None."""
+    if flux == "fused":
+        name, key = "stage_kernel_dram.json", None
+    elif flux == "per_cell":
+        name, key = "split_stage_dram.json", precision
+    else:
+        return None
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
-    return d.get("dram_bytes_per_cell_per_launch", 0) * cells or None
+    if key is None:
+        per = d.get("dram_bytes_per_cell_per_launch") if precision == "fp64" else None
+    else:
+        per = d.get("dram_bytes_per_cell_per_stage", {}).get(key)
+    return per * cells if per else None
 
 
 BATCH_SIDES = (81, 121, 161, 201)
@@ -421,7 +431,7 @@ def run_vah(args, rank, world, dist):
                        "faces": args.flux,
                        "autotune": {k: c for k, c in zip(("face_x", "face_y", "face_z", "cell"), tune)}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic_per_launch(cells),
+                         "frac": achieved / peak, "traffic": traffic_per_launch(cells, args.flux, args.precision),
                          "peak_kind": f"{peak_kind} copy bandwidth",
                          "algorithmic_bytes_per_cell_update": bpc,
                          "kernel": ("stage_kernel (one fused RK stage)" if args.flux == "fused"
