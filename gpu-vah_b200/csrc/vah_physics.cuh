@@ -203,10 +203,15 @@ VAH_HD double approx_derivative(double x, double y, double z) {
 // Conserved (T^{tau mu}, P_L, pi^{tau mu}, Pi) -> (e, p, u^mu) by Newton on
 // u_T (EnergyMomentumTensor.cpp:30-197): relative tolerance 1e-7, at most
 // 10^4 iterations; on failure e = 0.999 ePrev, u = (1,0,0,0).
-// Returns 0 (converged), 1 (fallback) or 2 (a NaN reached e or u).
-// out = {e, p, ut, ux, uy, un}.
+//
+// The guess-independent part (InvSetup) is split from the iteration so that a
+// face, inverted from both neighbours' guesses, sets up each state once.
+struct InvSetup {
+    double pl, bulk, m0, m1, m2, m3, F, x, mbt, bT, bL, b, c0;
+};
+
 template <int PHYS>
-VAH_HD int invert(const Eos &eos, double t, const double *q, double ePrev, double uT0, double *out) {
+VAH_HD void invert_setup(double t, const double *q, InvSetup &s) {
     double pitt = 0, pitx = 0, pity = 0, pitn = 0, bulk = 0;
     if (Phys<PHYS>::PIMUNU) {
         pitt = q[5];
@@ -225,19 +230,33 @@ VAH_HD int invert(const Eos &eos, double t, const double *q, double ePrev, doubl
     const double x = sqrt(fabs(1. - Ft2));
     double mbt = sqrt(m1 * m1 + m2 * m2);
     if (mbt == 0.0) mbt = 1.e-16;
+    s.pl = pl;
+    s.bulk = bulk;
+    s.m0 = m0;
+    s.m1 = m1;
+    s.m2 = m2;
+    s.m3 = m3;
+    s.F = F;
+    s.x = x;
+    s.mbt = mbt;
+    s.bT = x * mbt;
+    s.bL = x * x * m0 - Ft2 * pl;
+    s.b = x * x + Ft2;
+    s.c0 = m0 - t * Ft * m3;
+}
 
-    const double bT = x * mbt;
-    const double bL = x * x * m0 - Ft2 * pl;
-    const double b = x * x + Ft2;
-    const double c0 = m0 - t * Ft * m3;
-    double w = uT0, uT = uT0;
-    int status = 1;
+// Newton iteration for u_T from the guess uT0 (EnergyMomentumTensor.cpp:30-72).
+// Returns 0 with the root in uT, or 1 when the reference falls back.
+VAH_HD int newton_uT(const InvSetup &s, double uT0, double &uT) {
+    const double x = s.x, mbt = s.mbt, bT = s.bT, bL = s.bL, b = s.b, c0 = s.c0, pl = s.pl, bulk = s.bulk;
+    double w = uT0;
+    uT = uT0;
     for (int it = 0; it < 10000; ++it) {
         const double w2 = 1 + w * w;
         const double r = rsqrt_d(w2);
         const double v = w * r;
         const double e = c0 - v * x * mbt;
-        if (e < 0.0) break;
+        if (e < 0.0) return 1;
         const double g = bL + b * (0.5 * (e - pl) + 1.5 * bulk);
         const double r3 = r * r * r;
         const double f = v * g - bT;
@@ -245,23 +264,31 @@ VAH_HD int invert(const Eos &eos, double t, const double *q, double ePrev, doubl
         if (fabs(fp) == 0.0) fp = 1.e-16;
         const double next = w - f / fp;
         uT = next;
-        if (isnan(next) || isinf(next) || next < 0 || next > 9.0072e+15) break;
-        if (fabs(next - w) <= 1.e-7 * fabs(next)) {
-            status = 0;
-            break;
-        }
+        if (isnan(next) || isinf(next) || next < 0 || next > 9.0072e+15) return 1;
+        if (fabs(next - w) <= 1.e-7 * fabs(next)) return 0;
         w = next;
     }
+    return 1;
+}
+
+// The full inversion. Returns 0 (converged), 1 (fallback) or 2 (a NaN
+// reached e or u). out = {e, p, ut, ux, uy, un}.
+template <int PHYS>
+VAH_HD int invert(const Eos &eos, double t, const double *q, double ePrev, double uT0, double *out) {
+    InvSetup s;
+    invert_setup<PHYS>(t, q, s);
+    double uT;
+    const int status = newton_uT(s, uT0, uT);
     double e, ut, ux, uy, un;
     if (status == 0) {
         const double C = sqrt(1.0 + uT * uT);
         const double U = uT / C;
-        const double inv_mbt = 1.0 / mbt, inv_x = 1.0 / x;
-        ux = uT * m1 * inv_mbt;
-        uy = uT * m2 * inv_mbt;
-        un = F * C * inv_x;
+        const double inv_mbt = 1.0 / s.mbt, inv_x = 1.0 / s.x;
+        ux = uT * s.m1 * inv_mbt;
+        uy = uT * s.m2 * inv_mbt;
+        un = s.F * C * inv_x;
         ut = C * inv_x;
-        e = c0 - U * x * mbt;
+        e = s.c0 - U * s.x * s.mbt;
     } else {
         e = ePrev * .999;
         ux = 0.0;
@@ -279,24 +306,55 @@ VAH_HD int invert(const Eos &eos, double t, const double *q, double ePrev, doubl
     return status;
 }
 
+// What a face needs of an inversion: the velocity v_dir = u^dir / u^tau
+// (u^tau = C/x, u^x = uT m1/mbt, u^y = uT m2/mbt, u^eta = F C/x with
+// C = sqrt(1 + uT^2), so v_x = uT m1 x / (mbt C), v_eta = F), 0 after a
+// fallback (u = (1,0,0,0)). Same statuses as invert; a fallback's NaN check
+// is on e = 0.999 ePrev, a converged one's on v and the energy offset.
+VAH_HD int face_velocity(const InvSetup &s, double ePrev, double uT0, int dir, double *v) {
+    double uT;
+    if (newton_uT(s, uT0, uT) != 0) {
+        *v = 0.0;
+        return isnan(ePrev) ? 2 : 1;
+    }
+    double vv;
+    if (dir == 2) {
+        vv = s.F;
+    } else {
+        const double C = sqrt(1.0 + uT * uT);
+        vv = uT * (dir == 0 ? s.m1 : s.m2) * s.x / (s.mbt * C);
+    }
+    *v = vv;
+    return (isnan(vv) || isnan(s.c0)) ? 2 : 0;
+}
+
 // ------------------------------------------------------------ face flux --
 // Kurganov-Tadmor central flux at one face from the reconstructed states
 // (SemiDiscreteKurganovTadmorScheme.cpp:13-57, SpectralRadius.cpp:14-24,
 // LocalPropagationSpeed.cpp:14-22, FluxFunctions.cpp:15-25):
 // H = (F(qR) + F(qL) - a (qR - qL)) / 2, F = v_dir q, a = max |v_dir|.
+// sR/sL: the inversion set-ups of qR/qL; ePrev, uT: the evaluating cell's
+// fallback energy and Newton guess.
 // Returns the number of the two inversions that fell back; bit 8 flags a NaN.
 template <int PHYS>
-VAH_HD int face_flux(const Eos &eos, double t, const double *qR, const double *qL, int dir, double ePrev,
-                     double uT, double *H) {
+VAH_HD int face_flux_setup(const InvSetup &sR, const InvSetup &sL, const double *qR, const double *qL, int dir,
+                           double ePrev, double uT, double *H) {
     constexpr int NQ = Phys<PHYS>::NQ;
-    double R[6], L[6];
-    const int sR = invert<PHYS>(eos, t, qR, ePrev, uT, R);
-    const int sL = invert<PHYS>(eos, t, qL, ePrev, uT, L);
-    const double vR = R[3 + dir] / R[2], vL = L[3 + dir] / L[2];
+    double vR, vL;
+    const int stR = face_velocity(sR, ePrev, uT, dir, &vR);
+    const int stL = face_velocity(sL, ePrev, uT, dir, &vL);
     const double a = fmax(fabs(vL), fabs(vR));
 #pragma unroll
     for (int n = 0; n < NQ; ++n) H[n] = 0.5 * (vR * qR[n] + vL * qL[n] - a * (qR[n] - qL[n]));
-    return (sR != 0) + (sL != 0) + ((sR == 2 || sL == 2) ? 256 : 0);
+    return (stR != 0) + (stL != 0) + ((stR == 2 || stL == 2) ? 256 : 0);
+}
+
+template <int PHYS>
+VAH_HD int face_flux(double t, const double *qR, const double *qL, int dir, double ePrev, double uT, double *H) {
+    InvSetup sR, sL;
+    invert_setup<PHYS>(t, qR, sR);
+    invert_setup<PHYS>(t, qL, sL);
+    return face_flux_setup<PHYS>(sR, sL, qR, qL, dir, ePrev, uT, H);
 }
 
 // ------------------------------------------------------- axis sources --

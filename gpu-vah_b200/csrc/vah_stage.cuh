@@ -108,7 +108,7 @@ VAH_HD unsigned axis_update(const StageArgs<S> &a, long long s, int dir, long lo
         qR[n] = qp - approx_derivative(qc[n], qp, qpp) * 0.5;
         qL[n] = qc[n] + approx_derivative(qm, qc[n], qp) * 0.5;
     }
-    fails += face_flux<PHYS>(a.eos, a.t_src, qR, qL, dir, ePrev, uT, H);
+    fails += face_flux<PHYS>(a.t_src, qR, qL, dir, ePrev, uT, H);
 #pragma unroll
     for (int n = 0; n < NQ; ++n) val[n] -= c * H[n];
     // face at -1/2: right state from this cell, left state from cell -1
@@ -118,7 +118,7 @@ VAH_HD unsigned axis_update(const StageArgs<S> &a, long long s, int dir, long lo
         qR[n] = qc[n] - approx_derivative(qm, qc[n], qp) * 0.5;
         qL[n] = qm + approx_derivative(qmm, qm, qc[n]) * 0.5;
     }
-    fails += face_flux<PHYS>(a.eos, a.t_src, qR, qL, dir, ePrev, uT, H);
+    fails += face_flux<PHYS>(a.t_src, qR, qL, dir, ePrev, uT, H);
 #pragma unroll
     for (int n = 0; n < NQ; ++n) val[n] += c * H[n];
     if (Phys<PHYS>::PIMUNU) {
@@ -226,13 +226,16 @@ VAH_HD unsigned face_compute(const StageArgs<S> &a, long long s, int dir, long l
         qR[n] = qp - approx_derivative(q0, qp, qpp) * 0.5;
         qL[n] = q0 + approx_derivative(qm, q0, qp) * 0.5;
     }
+    InvSetup sR, sL;  // set up once, inverted from one guess (shared) or both (reference faces)
+    invert_setup<PHYS>(a.t_src, qR, sR);
+    invert_setup<PHYS>(a.t_src, qL, sL);
     const double ux = ld(a.uin[1], s), uy = ld(a.uin[2], s);
-    unsigned fails = face_flux<PHYS>(a.eos, a.t_src, qR, qL, dir, ld(a.ein, s), sqrt(fabs(ux * ux + uy * uy)), H);
+    unsigned fails = face_flux_setup<PHYS>(sR, sL, qR, qL, dir, ld(a.ein, s), sqrt(fabs(ux * ux + uy * uy)), H);
 #pragma unroll
     for (int n = 0; n < NQ; ++n) a.H[dir][n][s] = (S)H[n];
     if (EXACT) {
         const double vx = ld(a.uin[1], s + st), vy = ld(a.uin[2], s + st);
-        fails += face_flux<PHYS>(a.eos, a.t_src, qR, qL, dir, ld(a.ein, s + st), sqrt(fabs(vx * vx + vy * vy)), H);
+        fails += face_flux_setup<PHYS>(sR, sL, qR, qL, dir, ld(a.ein, s + st), sqrt(fabs(vx * vx + vy * vy)), H);
 #pragma unroll
         for (int n = 0; n < NQ; ++n) a.HR[dir][n][s] = (S)H[n];
     }
