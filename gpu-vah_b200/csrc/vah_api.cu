@@ -8,6 +8,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -40,6 +41,7 @@ struct vah_event {
     unsigned long long *d_counters;  // face fallbacks, cell fallbacks, NaN cells
     long long steps;
     double last_t, last_dt;          // time and step of the latest vah_rk2_step (autotuning state)
+    double *d_stage64;               // FP32 storage: one FP64 field of staging for the host-buffer step
     vah::SplitConfig split;          // launch configuration of the face/cell kernels
     bool timing;
     std::vector<cudaEvent_t> tev;  // start/stop pairs of timed launches
@@ -97,6 +99,7 @@ void free_all(vah_event *ev) {
     cudaFree(ev->d_tab);
     cudaFree(ev->d_exc);
     cudaFree(ev->d_counters);
+    cudaFree(ev->d_stage64);
     for (cudaEvent_t e : ev->tev) cudaEventDestroy(e);
     if (ev->own_stream && ev->stream) cudaStreamDestroy(ev->stream);
 }
@@ -197,6 +200,7 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->timing = false;
     ev->steps = 0;
     ev->last_t = hydro->t0;
+    ev->d_stage64 = nullptr;
     ev->last_dt = 0.005;
     ev->split = vah::default_split_config();
     ev->nexc = 0;
@@ -596,20 +600,51 @@ extern "C" int vah_event_kernel_time(vah_event *ev, double *ms, long long *launc
     return VAH_OK;
 }
 
+namespace {
+
+__global__ void widen_kernel(const float *__restrict__ src, double *__restrict__ dst, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        dst[k] = (double)src[k];
+}
+
+__global__ void narrow_kernel(const double *__restrict__ src, float *__restrict__ dst, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        dst[k] = (float)src[k];
+}
+
+// FP32 storage: the caller's FP64 host arrays cross PCIe as FP64 into one
+// field of device staging and are narrowed (widened on the way out) by a
+// kernel, all in stream order, with one synchronisation at the end.
+int step_host_fp32(vah_event *ev, double t, double dt, double *const *fields) {
+    const size_t n = ev->ncell;
+    if (!ev->d_stage64) VAH_TRY(cudaMalloc((void **)&ev->d_stage64, n * sizeof(double)));
+    const int block = 256, grid = (int)std::min<size_t>((n + block - 1) / block, 148 * 16);
+    for (int id = 0; id < VAH_NUM_FIELDS; ++id) {
+        float *d = (float *)field_ptr(ev, id);
+        if (!d || !fields[id]) continue;
+        VAH_TRY(cudaMemcpyAsync(ev->d_stage64, fields[id], n * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
+        narrow_kernel<<<grid, block, 0, ev->stream>>>(ev->d_stage64, d, n);
+        VAH_TRY(cudaGetLastError());
+    }
+    int rc = vah_rk2_step(ev, t, dt);
+    if (rc != VAH_OK) return rc;
+    for (int id = 0; id < VAH_NUM_FIELDS; ++id) {  // pointers after the u <-> up swap
+        const float *d = (const float *)field_ptr(ev, id);
+        if (!d || !fields[id]) continue;
+        widen_kernel<<<grid, block, 0, ev->stream>>>(d, ev->d_stage64, n);
+        VAH_TRY(cudaGetLastError());
+        VAH_TRY(cudaMemcpyAsync(fields[id], ev->d_stage64, n * sizeof(double), cudaMemcpyDeviceToHost, ev->stream));
+    }
+    return vah_event_sync(ev);
+}
+
+}  // namespace
+
 extern "C" int vah_rk2_step_host(vah_event *ev, double t, double dt, double *const *fields) {
     if (!ev || !fields) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(ev->opt.device));
     int rc;
-    if (ev->elem != sizeof(double)) {  // FP32 storage: converting copies
-        for (int id = 0; id < VAH_NUM_FIELDS; ++id)
-            if (field_ptr(ev, id) && fields[id] && (rc = vah_event_set_field(ev, id, fields[id], 1)) != VAH_OK)
-                return rc;
-        if ((rc = vah_rk2_step(ev, t, dt)) != VAH_OK || (rc = vah_event_sync(ev)) != VAH_OK) return rc;
-        for (int id = 0; id < VAH_NUM_FIELDS; ++id)
-            if (field_ptr(ev, id) && fields[id] && (rc = vah_event_get_field(ev, id, fields[id], 1)) != VAH_OK)
-                return rc;
-        return VAH_OK;
-    }
+    if (ev->elem != sizeof(double)) return step_host_fp32(ev, t, dt, fields);
     const size_t bytes = ev->ncell * sizeof(double);
     // all copies are queued on the event's stream; one synchronisation at the end
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {

@@ -215,7 +215,10 @@ int vah_event_autotune(vah_event *ev, int reps, vah_tune_report *out);
  * full ghosted layout) are copied in, stepped once on the GPU, and copied
  * back. Drop-in for rungeKutta2 on host arrays
  * (FullyDiscreteKurganovTadmorScheme.h:13-15). `fields` holds
- * VAH_NUM_FIELDS pointers; unused physics slots may be NULL. */
+ * VAH_NUM_FIELDS pointers; unused physics slots may be NULL. With FP32
+ * storage the arrays still cross as FP64 and are narrowed (widened on the
+ * way back) by a kernel, through one field of device staging that the first
+ * such call allocates. */
 int vah_rk2_step_host(vah_event *ev, double t, double dt, double *const *fields);
 
 /* ---- batches: many events of uneven size in one launch per kernel kind ----

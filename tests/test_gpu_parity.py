@@ -180,6 +180,29 @@ def test_gpu_host_buffer_step_matches_device_step():
     ev.close()
 
 
+def test_gpu_host_buffer_step_fp32_storage_matches_device_step():
+    """FP32 storage: the host-buffer step narrows and widens on the device;
+    the result equals set_field + step + get_field bit for bit."""
+    g, e2 = conformal_workload(21, 19)
+    ev = V.Event(g, t0=0.5, precision=1)
+    ev.init_from_e(0.5, e2, 1)
+    ev.run(0.5, 0.02, 3)
+    ids = [fid for fid in range(V.NUM_FIELDS) if fid < 15 or fid >= 16]
+    state0 = {fid: ev.get_field(fid) for fid in ids}
+    state = {fid: a.copy() for fid, a in state0.items()}
+    ptrs = [state[fid].ctypes.data if fid in state else 0 for fid in range(V.NUM_FIELDS)]
+    ev.step_host(0.56, 0.02, ptrs)
+    ev.step_host(0.58, 0.02, ptrs)
+    dev = V.Event(g, t0=0.5, precision=1)
+    upload(dev, g, state0)
+    dev.step(0.56, 0.02)
+    dev.step(0.58, 0.02)
+    for fid in ids:
+        np.testing.assert_array_equal(state[fid], dev.get_field(fid), err_msg=f"field {fid}")
+    dev.close()
+    ev.close()
+
+
 def test_gpu_nan_is_reported_not_fatal():
     g, e2 = conformal_workload(9, 9)
     ev = V.Event(g, t0=0.5)
