@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -35,6 +36,9 @@ struct SlotDesc {
     S *q[16], *qS[16], *ep[2][2], *uA[4], *uB[4], *uS[4];
     S *H[3][16], *HR[3][16];
     unsigned char *fallback;  // per ghosted cell: 1 where the latest cell inversion fell back
+    unsigned char *hot;       // per ghosted cell: 1 while e > e_freeze (freeze-out crossings)
+    double e_freeze;
+    unsigned long long *crossings;  // [down, up] during the current step
     unsigned long long *counters;
 };
 
@@ -71,6 +75,9 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
     a.eos = eos;
     a.counters = d.counters;
     a.fallback = d.fallback;
+    a.hot = d.hot;
+    a.e_freeze = d.e_freeze;
+    a.crossings = d.crossings;
     S *const *u = c.parity ? d.uB : d.uA;
     S *const *up = c.parity ? d.uA : d.uB;
     for (int n = 0; n < 16; ++n) {
@@ -137,12 +144,30 @@ __global__ void __launch_bounds__(kTX *kTY, MINB) batch_kernel(const SlotDesc<S>
     }
 }
 
-__global__ void advance_kernel(SlotClock *clk, const double *dts, int nslots) {
+// End of a step: the clock moves on, and the freeze-out surface volume takes
+// the step's net crossings (down - up) times tau dx dy deta at the new time.
+__global__ void advance_kernel(SlotClock *clk, const double *dts, int nslots, unsigned long long *cross, double *vol,
+                               const double *dv) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < nslots && clk[s].active) {
-        clk[s].t += dts[s];
+        const double t_new = clk[s].t + dts[s];
+        const double net = (double)cross[2 * s] - (double)cross[2 * s + 1];
+        if (net != 0.0) vol[s] += t_new * net * dv[s];
+        cross[2 * s] = cross[2 * s + 1] = 0;
+        clk[s].t = t_new;
         clk[s].parity ^= 1;
         clk[s].steps += 1;
+    }
+}
+
+// Freeze-out state at admission: 1 where the interior e exceeds e_freeze.
+template <typename S>
+__global__ void hot_init_kernel(const S *e, unsigned char *hot, double e_freeze, int nx, int ny, int nz) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+        const long long s = (i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * (k + 2));
+        hot[s] = (double)e[s] > e_freeze;
     }
 }
 
@@ -175,8 +200,9 @@ __global__ void max_e_kernel(const SlotDesc<S> *__restrict__ descs, const WorkIt
 }
 
 // Per-tile partial sums of the event observables (tau T^tt, T^xx - T^yy,
-// T^xx + T^yy, e u^t u_T, e u^t) in FP64, one row per cell tile; the host
-// adds the rows of each slot in a fixed order.
+// T^xx + T^yy, e u^t u_T, e u^t) in FP64 over the cells whose latest
+// inversion converged (a fallback cell's state is not a solution), one row
+// per cell tile; the host adds the rows of each slot in a fixed order.
 template <typename S, int PHYS>
 __global__ void observables_kernel(const SlotDesc<S> *__restrict__ descs, const SlotClock *__restrict__ clk,
                                    const WorkItem *__restrict__ work, int nwork, double *partial) {
@@ -188,9 +214,10 @@ __global__ void observables_kernel(const SlotDesc<S> *__restrict__ descs, const 
         const SlotClock c = clk[it.slot];
         const int i = it.i0 + threadIdx.x, r = it.r0 + threadIdx.y;
         double acc[5] = {0, 0, 0, 0, 0};
-        if (i < d.nx && r < d.ny * d.nz) {
-            const int j = r % d.ny, k = r / d.ny;
-            const long long s = (i + 2) + (long long)d.ncx * (j + 2) + d.plane * (k + 2);
+        const bool in = i < d.nx && r < d.ny * d.nz;
+        const int j = in ? r % d.ny : 0, k = in ? r / d.ny : 0;
+        const long long s = (i + 2) + (long long)d.ncx * (j + 2) + d.plane * (k + 2);
+        if (in && !d.fallback[s]) {  // converged cells only
             S *const *u = c.parity ? d.uB : d.uA;
             const double e = (double)d.ep[0][0][s], p = (double)d.ep[0][1][s], pl = (double)d.q[kSlotPL][s];
             const double ut = (double)u[0][s], ux = (double)u[1][s], uy = (double)u[2][s];
@@ -292,6 +319,10 @@ struct vah_batch {
     void *d_desc;               // SlotDesc<S>[kMaxSlots]
     SlotClock *d_clk;           // [kMaxSlots]
     double *d_dt;               // [kMaxSlots]
+    unsigned long long *d_cross;  // [kMaxSlots * 2] freeze-out crossings of the current step (down, up)
+    double *d_vol;              // [kMaxSlots] freeze-out surface volume so far, fm^4
+    double *d_dv;               // [kMaxSlots] dx dy deta
+    std::vector<double> tab;    // host copy of the EoS table (freeze-out energy densities)
     unsigned long long *d_counters;  // [kMaxSlots * 4]
     unsigned long long *d_maxbits;   // [kMaxSlots]
     struct Slot {
@@ -338,7 +369,7 @@ int nq_of(int physics) { return physics == VAH_IDEAL ? 5 : (physics == VAH_PIMUN
 
 // Arrays of one event in its allocation: 16 q, 16 qS, 4 e/p, 4 uA, 4 uB,
 // 4 uS, and the face buffers (H, plus HR for reference faces) per axis; then
-// one byte per cell of fallback flags.
+// one byte per cell of fallback flags and one of freeze-out state.
 int arrays_per_event(const vah_batch *b, const vah_lattice *lat) {
     const int ndir = lat->nz > 1 ? 3 : 2;
     const int per_face = b->opt.flux == VAH_FLUX_PER_CELL ? 2 : 1;
@@ -348,7 +379,7 @@ int arrays_per_event(const vah_batch *b, const vah_lattice *lat) {
 size_t event_bytes(const vah_batch *b, const vah_lattice *lat) {
     const size_t ncell = (size_t)(lat->nx + 4) * (lat->ny + 4) * (lat->nz + 4);
     const size_t per = (ncell * b->elem + 255) / 256 * 256;
-    return per * arrays_per_event(b, lat) + (ncell + 255) / 256 * 256 + 256;
+    return per * arrays_per_event(b, lat) + 2 * ((ncell + 255) / 256 * 256) + 256;
 }
 
 vah::Eos batch_eos(const vah_batch *b) {
@@ -364,6 +395,25 @@ vah::Eos batch_eos(const vah_batch *b) {
 template <typename S>
 SlotDesc<S> *desc_host(vah_batch *b, int slot) {
     return (SlotDesc<S> *)b->desc_host.data() + slot;
+}
+
+// Energy density at temperature T (fm^-1): the conformal gas e = 13.8997 T^4
+// (EquationOfState.cpp:144 inverted) or the table's monotone T(e), bisected
+// in ln e.
+double energy_at_temperature(const vah_batch *b, double T) {
+    if (b->opt.eos != VAH_EOS_TABLE || b->tab.empty()) return 13.8997 * T * T * T * T;
+    const int n = (int)b->tab[0];
+    const double *Tt = b->tab.data() + VAH_EOS_TABLE_HEADER + n;
+    if (T <= Tt[0]) return b->tab[4];
+    if (T >= Tt[n - 1]) return b->tab[6];
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (Tt[mid] < T) lo = mid;
+        else hi = mid;
+    }
+    const double w = (T - Tt[lo]) / (Tt[hi] - Tt[lo]);
+    return std::exp(b->tab[1] + b->tab[3] * (lo + w));
 }
 
 template <typename S>
@@ -406,6 +456,9 @@ int fill_slot(vah_batch *b, int slot) {
             if (b->opt.flux == VAH_FLUX_PER_CELL) d.HR[k][n] = next();
         }
     d.fallback = (unsigned char *)(base + off);
+    d.hot = (unsigned char *)(base + off + (ncell + 255) / 256 * 256);
+    d.e_freeze = energy_at_temperature(b, sl.hydro.freezeout_T_GeV / 0.197326938);
+    d.crossings = b->d_cross + 2 * slot;
     *desc_host<S>(b, slot) = d;
     VAH_TRY(cudaMemcpyAsync((char *)b->d_desc + sizeof(SlotDesc<S>) * slot, &d, sizeof(d), cudaMemcpyHostToDevice,
                             b->stream));
@@ -474,7 +527,8 @@ int enqueue_step(vah_batch *b) {
     const Eos eos = batch_eos(b);
     for (int stage = 1; stage <= 2; ++stage)
         for (int kind = 0; kind < K_NUM; ++kind) VAH_TRY((launch_kind_rt<S, PHYS, EXACT>(b, descs, kind, stage, eos)));
-    advance_kernel<<<(kMaxSlots + 255) / 256, 256, 0, b->stream>>>(b->d_clk, b->d_dt, kMaxSlots);
+    advance_kernel<<<(kMaxSlots + 255) / 256, 256, 0, b->stream>>>(b->d_clk, b->d_dt, kMaxSlots, b->d_cross, b->d_vol,
+                                                                 b->d_dv);
     VAH_TRY(cudaGetLastError());
     return VAH_OK;
 }
@@ -550,6 +604,13 @@ int init_slot(vah_batch *b, int slot, double t0, const double *e_interior, int p
     VAH_TRY(cudaMemcpyAsync(b->d_clk + slot, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
     VAH_TRY(cudaMemcpyAsync(b->d_dt + slot, &sl.dt, sizeof(double), cudaMemcpyHostToDevice, b->stream));
     VAH_TRY(cudaMemsetAsync(b->d_counters + 4 * slot, 0, 4 * sizeof(unsigned long long), b->stream));
+    VAH_TRY(cudaMemsetAsync(b->d_cross + 2 * slot, 0, 2 * sizeof(unsigned long long), b->stream));
+    VAH_TRY(cudaMemsetAsync(b->d_vol + slot, 0, sizeof(double), b->stream));
+    const double dv = sl.lat.dx * sl.lat.dy * sl.lat.dz;
+    VAH_TRY(cudaMemcpyAsync(b->d_dv + slot, &dv, sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    vah::hot_init_kernel<S><<<std::max(1, std::min(nx * ny * nz / 256 + 1, 148 * 16)), 256, 0, b->stream>>>(
+        d.ep[0][0], d.hot, d.e_freeze, nx, ny, nz);
+    VAH_TRY(cudaGetLastError());
     VAH_TRY(cudaStreamSynchronize(b->stream));  // the staging vector dies here
     return VAH_OK;
 }
@@ -610,17 +671,24 @@ extern "C" int vah_batch_create(const vah_options *opt, const double *eos_table,
     chk(cudaMalloc(&b->d_desc, desc_size * vah::kMaxSlots));
     chk(cudaMalloc((void **)&b->d_clk, sizeof(SlotClock) * vah::kMaxSlots));
     chk(cudaMalloc((void **)&b->d_dt, sizeof(double) * vah::kMaxSlots));
+    chk(cudaMalloc((void **)&b->d_cross, sizeof(unsigned long long) * 2 * vah::kMaxSlots));
+    chk(cudaMalloc((void **)&b->d_vol, sizeof(double) * vah::kMaxSlots));
+    chk(cudaMalloc((void **)&b->d_dv, sizeof(double) * vah::kMaxSlots));
     chk(cudaMalloc((void **)&b->d_counters, sizeof(unsigned long long) * 4 * vah::kMaxSlots));
     chk(cudaMalloc((void **)&b->d_maxbits, sizeof(unsigned long long) * vah::kMaxSlots));
     if (rc == VAH_OK) {
         chk(cudaMemset(b->d_clk, 0, sizeof(SlotClock) * vah::kMaxSlots));
         chk(cudaMemset(b->d_dt, 0, sizeof(double) * vah::kMaxSlots));
         chk(cudaMemset(b->d_counters, 0, sizeof(unsigned long long) * 4 * vah::kMaxSlots));
+        chk(cudaMemset(b->d_cross, 0, sizeof(unsigned long long) * 2 * vah::kMaxSlots));
+        chk(cudaMemset(b->d_vol, 0, sizeof(double) * vah::kMaxSlots));
+        chk(cudaMemset(b->d_dv, 0, sizeof(double) * vah::kMaxSlots));
     }
     if (rc == VAH_OK && opt->eos == VAH_EOS_TABLE) {
         const size_t len = VAH_EOS_TABLE_LEN((size_t)eos_table[0]);
         chk(cudaMalloc((void **)&b->d_tab, len * sizeof(double)));
         chk(cudaMemcpy(b->d_tab, eos_table, len * sizeof(double), cudaMemcpyHostToDevice));
+        b->tab.assign(eos_table, eos_table + len);
     }
     if (rc == VAH_OK && opt->eos == VAH_EOS_CONFORMAL) {
         const std::vector<uint32_t> &exc = vah::powf_quarter_exceptions();
@@ -656,6 +724,9 @@ extern "C" int vah_batch_destroy(vah_batch *b) {
     cudaFree(b->d_desc);
     cudaFree(b->d_clk);
     cudaFree(b->d_dt);
+    cudaFree(b->d_cross);
+    cudaFree(b->d_vol);
+    cudaFree(b->d_dv);
     cudaFree(b->d_counters);
     cudaFree(b->d_maxbits);
     cudaFree(b->d_tab);
@@ -768,6 +839,11 @@ extern "C" int vah_batch_event_info(vah_batch *b, int slot, vah_event_info *out)
     return VAH_OK;
 }
 
+template <typename S>
+const unsigned char *slot_fallback(vah_batch *b, int slot) {
+    return desc_host<S>(b, slot)->fallback;
+}
+
 extern "C" int vah_batch_get_field(vah_batch *b, int slot, int field, double *host, int with_ghosts) {
     if (!b || !host || slot < 0 || slot >= vah::kMaxSlots || !b->slots[slot].used) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(b->opt.device));
@@ -796,6 +872,29 @@ extern "C" int vah_batch_get_field(vah_batch *b, int slot, int field, double *ho
     VAH_TRY(cudaStreamSynchronize(b->stream));
     if (es == sizeof(float))
         for (size_t k = 0; k < n; ++k) host[k] = (double)f32[k];
+    return VAH_OK;
+}
+
+extern "C" int vah_batch_fallback_mask(vah_batch *b, int slot, unsigned char *host) {
+    if (!b || !host || slot < 0 || slot >= vah::kMaxSlots || !b->slots[slot].used) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(b->opt.device));
+    const vah_lattice &lat = b->slots[slot].lat;
+    const size_t ncx = lat.nx + 4, ncy = lat.ny + 4;
+    const unsigned char *src = b->elem == sizeof(float) ? slot_fallback<float>(b, slot) : slot_fallback<double>(b, slot);
+    for (int k = 0; k < lat.nz; ++k)
+        VAH_TRY(cudaMemcpy2DAsync(host + (size_t)lat.nx * lat.ny * k, lat.nx, src + 2 + ncx * (2 + ncy * (k + 2)), ncx,
+                                  lat.nx, lat.ny, cudaMemcpyDeviceToHost, b->stream));
+    VAH_TRY(cudaStreamSynchronize(b->stream));
+    return VAH_OK;
+}
+
+extern "C" int vah_batch_freezeout_volume(vah_batch *b, double *out, int nslots) {
+    if (!b || !out || nslots < 0 || nslots > vah::kMaxSlots) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(b->opt.device));
+    VAH_TRY(cudaStreamSynchronize(b->stream));
+    if (nslots) VAH_TRY(cudaMemcpy(out, b->d_vol, sizeof(double) * nslots, cudaMemcpyDeviceToHost));
+    for (int s = 0; s < nslots; ++s)
+        if (s >= (int)b->slots.size() || !b->slots[s].used) out[s] = 0.0;
     return VAH_OK;
 }
 

@@ -38,6 +38,11 @@ struct StageArgs {
     Eos eos;
     unsigned long long *counters;  // [face fallbacks, cell fallbacks, NaN cells]
     unsigned char *fallback;       // optional: per ghosted cell, 1 where this stage's inversion fell back
+    // optional freeze-out crossing test at the end of a step (stage 2): per
+    // ghosted cell 1 while e > e_freeze; crossings counted [down, up]
+    unsigned char *hot;
+    double e_freeze;
+    unsigned long long *crossings;
     // face/cell split: flux through the face at +1/2 of ghosted cell s along
     // axis d, field n, as cell s evaluates it (H) and as cell s+1 does (HR,
     // reference face semantics only); scratch of ncell entries per field
@@ -291,6 +296,13 @@ VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
     if (st != 0 && a.counters) count_add(a.counters + 1, 1ull);
     if ((bad || st == 2) && a.counters) count_add(a.counters + 2, 1ull);
     if (a.fallback) a.fallback[s] = st != 0;
+    if (a.hot && a.stage2 && st == 0) {  // the isotherm e = e_freeze passed this (converged) cell during the step
+        const unsigned char was = a.hot[s], now = e > a.e_freeze;
+        if (was != now) {
+            a.hot[s] = now;
+            count_add(a.crossings + (was ? 0 : 1), 1ull);
+        }
+    }
     store_cell(a, s, NQ, val, u, e, p);
     const long long sy = a.ncx, sz = a.plane;
     if (i == 2) { store_cell(a, s - 1, NQ, val, u, e, p); store_cell(a, s - 2, NQ, val, u, e, p); }

@@ -27,8 +27,12 @@ def rbar0(a):
     return np.polyval(RBAR0_NUM[::-1], a) / np.polyval(RBAR0_DEN[::-1], a)
 
 
-def observables(get, tau, dx, dy, dz, physics):
-    """get(field_id) -> interior array (float64)."""
+def observables(get, tau, dx, dy, dz, physics, mask=None):
+    """get(field_id) -> interior array (float64); mask: the cells to sum over
+    (all when None; the batch reductions sum over converged cells)."""
+    if mask is not None:
+        full = get
+        get = lambda f: full(f)[mask]  # noqa: E731
     e, p, pl = get(F_E), get(F_P), get(F_PL)
     ut, ux, uy = get(F_UT), get(F_UX), get(F_UY)
     bulk = get(F_PI) if physics == 2 else 0.0

@@ -74,7 +74,8 @@ EXPORTS = ["vah_version", "vah_eos_table_build", "vah_event_create", "vah_event_
            "vah_event_get_field", "vah_event_set_conserved", "vah_event_init_from_e", "vah_event_set_ghost_cells",
            "vah_rk2_step", "vah_run", "vah_event_sync", "vah_event_stats", "vah_event_set_timing",
            "vah_event_kernel_time", "vah_rk2_step_host", "vah_ic_optical_glauber", "vah_ic_mc_glauber",
-           "vah_ic_longitudinal", "vah_event_autotune", "vah_batch_autotune"]
+           "vah_ic_longitudinal", "vah_event_autotune", "vah_batch_autotune",
+           "vah_batch_freezeout_volume", "vah_batch_fallback_mask"]
 
 _lib = None
 
@@ -343,6 +344,19 @@ class Batch:
         out = np.zeros(3 * nslots)
         check(self.L.vah_batch_observables(self.b, out.ctypes.data_as(P), nslots), "vah_batch_observables")
         return out.reshape(nslots, 3)
+
+    def freezeout_volume(self, nslots):
+        """Per-slot freeze-out surface volume so far (fm^4)."""
+        out = np.zeros(nslots)
+        check(self.L.vah_batch_freezeout_volume(self.b, out.ctypes.data_as(P), nslots), "vah_batch_freezeout_volume")
+        return out
+
+    def fallback_mask(self, slot):
+        """Interior cells whose latest inversion fell back (bool array, x fastest)."""
+        nx, ny, nz = self.shapes[slot]
+        out = np.zeros(nx * ny * nz, np.uint8)
+        check(self.L.vah_batch_fallback_mask(self.b, slot, out.ctypes.data_as(C.c_void_p)), "vah_batch_fallback_mask")
+        return out.astype(bool)
 
     def set_timing(self, on):
         check(self.L.vah_batch_set_timing(self.b, int(on)), "vah_batch_set_timing")

@@ -264,11 +264,24 @@ int vah_batch_get_field(vah_batch *b, int slot, int field, double *host, int wit
  * deterministic. */
 int vah_batch_max_energy_density(vah_batch *b, double *out, int nslots);
 /* Per-slot observables in FP64 with a fixed summation order (an event's
- * values do not depend on the other events in the batch): out[3 s + 0] =
+ * values do not depend on the other events in the batch), over the interior
+ * cells whose latest inversion converged: out[3 s + 0] =
  * sum tau T^{tau tau} dx dy deta, out[3 s + 1] = eps_p =
  * sum(T^xx - T^yy)/sum(T^xx + T^yy), out[3 s + 2] = <u_T> = sum e u^tau u_T /
  * sum e u^tau. */
 int vah_batch_observables(vah_batch *b, double *out, int nslots);
+/* Per-slot freeze-out surface volume so far (fm^4; no reference counterpart,
+ * the reference reads freezeoutTemperatureGeV but never uses it,
+ * HydroPlugin.cpp:154-158): at the end of every step each cell whose
+ * inversion converged and whose e fell through e(T_f) adds tau dx dy deta at
+ * the new time, and each that rose through it subtracts the same, so a surface
+ * swept once counts once (a cell in the fallback keeps its state). Crossings
+ * are integer counts, so the value is deterministic. T_f is the event's
+ * vah_hydro.freezeout_T_GeV. out[s] = 0 for free slots. */
+int vah_batch_freezeout_volume(vah_batch *b, double *out, int nslots);
+/* Interior cells (nx*ny*nz, x fastest) whose latest inversion fell back to
+ * the reference's e = 0.999 e_prev, u = (1,0,0,0): 1, else 0. */
+int vah_batch_fallback_mask(vah_batch *b, int slot, unsigned char *host);
 int vah_batch_set_timing(vah_batch *b, int on);
 int vah_batch_kernel_time(vah_batch *b, double *ms, long long *steps);
 /* Register-cap autotuning of the batch's launch kinds (face x, y, z, cell

@@ -108,12 +108,55 @@ def test_batch_reductions_match_host():
     emax = batch.max_energy_density(n)
     obs = batch.observables(n)
     for slot, (nx, ny, nz, dx, dz, b, seed, dt) in zip(slots, EVENTS):
+        fell = batch.fallback_mask(slot)  # cells in the inversion fallback are left out of the reductions
         get = lambda f: batch.get_field(slot, f, False)
-        # cells in the inversion fallback (u = (1,0,0,0) exactly) are left out of the maximum
-        fell = (get(18) == 1.0) & (get(19) == 0.0) & (get(20) == 0.0) & (get(21) == 0.0)
         assert emax[slot] == np.max(np.where(fell, 0.0, get(16)))
-        host = OBS.observables(get, 0.4 + 5 * dt, dx, dx, dz, 2)
+        host = OBS.observables(get, 0.4 + 5 * dt, dx, dx, dz, 2, mask=~fell)
         assert abs(obs[slot, 0] / host["E_tot"] - 1) < 1e-12
         assert abs(obs[slot, 1] - host["eps_p"]) < 1e-12 * max(1, abs(host["eps_p"]))
         assert abs(obs[slot, 2] / host["uT_mean"] - 1) < 1e-12
     batch.close()
+
+
+def test_freezeout_volume_of_a_uniform_box_is_exact():
+    """A uniform 2+1D box stays uniform (zero-gradient ghosts), so every cell
+    crosses e(T_f) in the same step: the surface volume is then exactly
+    tau_f * N * dx dy deta, zero before, and unchanged after."""
+    tab = V.eos_table()
+    ef = vah.table_energy_density(tab, 0.15 / vah.HBARC)
+    nx, ny, dx, dz, t0, dt = 24, 20, 0.3, 0.2, 0.5, 0.02
+    batch = vah.Batch(table=tab)
+    slot = batch.add(nx, ny, 1, dx, dx, dz, t0, dt, 0.16, np.full(nx * ny, 3.0 * ef))
+    t, e_before, vol = t0, 3.0 * ef, 0.0
+    for n in range(400):
+        batch.step(1)
+        t = t + dt
+        vol = batch.freezeout_volume(slot + 1)[slot]
+        e = batch.get_field(slot, 16, False)
+        assert np.all(e == e[0])
+        if vol != 0.0:
+            break
+        e_before = e[0]
+    assert vol == t * float(nx * ny) * (dx * dx * dz), (n, vol)
+    # the step that crossed took e from above the freeze-out energy density to below it
+    assert e_before > ef * (1 - 1e-9) and e[0] <= ef * (1 + 1e-9)
+    batch.step(20)
+    assert batch.freezeout_volume(slot + 1)[slot] == vol  # swept once, counted once
+    batch.close()
+
+
+def test_freezeout_volume_does_not_depend_on_the_mix():
+    tab = V.eos_table()
+    mixed, alone = vah.Batch(table=tab), vah.Batch(table=tab)
+    slots = [mixed.add(nx, ny, nz, dx, dx, dz, 0.4, dt, 0.16, event_e(tab, nx, ny, nz, dx, dz, b, seed))
+             for (nx, ny, nz, dx, dz, b, seed, dt) in EVENTS]
+    nx, ny, nz, dx, dz, b, seed, dt = EVENTS[0]
+    s1 = alone.add(nx, ny, nz, dx, dx, dz, 0.4, dt, 0.16, event_e(tab, nx, ny, nz, dx, dz, b, seed))
+    mixed.step(60)
+    alone.step(60)
+    v_mix = mixed.freezeout_volume(max(slots) + 1)
+    v_alone = alone.freezeout_volume(s1 + 1)
+    assert v_mix[slots[0]] == v_alone[s1]
+    assert np.all(v_mix[slots] >= 0.0)
+    mixed.close()
+    alone.close()
