@@ -65,6 +65,14 @@ extern "C" void vref_free(void) {
     g_len = 0;
 }
 
+/* The reference's validity arrays (VALIDITY_DOMAIN, DynamicalVariables.h:86-117),
+ * member k in declaration order; checkValidity fills them at the end of every
+ * rungeKutta2 (FullyDiscreteKurganovTadmorScheme.cpp:791). */
+extern "C" PRECISION *vref_validity(int k) {
+    if (!validityDomain || k < 0 || (size_t)k >= sizeof(VALIDITY_DOMAIN) / sizeof(PRECISION *)) return 0;
+    return ((PRECISION **)validityDomain)[k];
+}
+
 /* Allocate the reference globals for an nx*ny*nz interior grid (2 ghost
  * layers per side, LatticeParameters.cpp:45-47). */
 extern "C" int vref_init(int nx, int ny, int nz, double dx, double dy, double dz,

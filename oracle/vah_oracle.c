@@ -34,6 +34,8 @@ struct vo_state {
     double *e, *p;
     double *u[4], *up[4], *uS[4];
     long long face_fail, cell_fail, nan_count;
+    int validity_on;
+    double *vd[VO_NUM_VALIDITY];
 };
 
 static int nq_of(int physics) {
@@ -690,7 +692,177 @@ static void regulate(vo_state *st, double t, double *const *q, double *const *u)
                 double fac = tanh(rho) / rho;
                 if (rho < 1.e-7) fac = 1.0;
                 for (int n = 5; n < 15; ++n) q[n][s] *= fac;
+                if (st->validity_on) {  /* :666-693: the factor, then each criterion's own factor */
+                    st->vd[16][s] = fac;
+                    for (int m = 0; m < 10; ++m) {
+                        double f = tanh(cand[m]) / cand[m];
+                        if (cand[m] < 1.e-7) f = 1.0;
+                        st->vd[17 + m][s] = f;
+                    }
+                }
             }
+}
+
+/* HydrodynamicValidity.cpp:47-394 at one interior cell: t = tau + dtau, qn =
+ * the conserved state at the start of the step (the reference passes q before
+ * it is swapped with Q), e, p, u the new primitives and up the previous u.
+ * Shear tensor and its transverse projection as in the source terms; the
+ * reference's later assignments of stt..snn (:197-200) are the ones kept. */
+static void validity_cell(vo_state *st, double t, double dt, double *const *qn, int s) {
+    const vo_config *c = &st->cfg;
+    double **v = st->vd;
+    const double e_s = st->e[s], p_s = st->p[s];
+    const double *U0 = st->u[0], *U1 = st->u[1], *U2 = st->u[2], *U3 = st->u[3];
+    const double ut = U0[s], ux = U1[s], uy = U2[s], un = U3[s];
+    const double utp = st->up[0][s], uxp = st->up[1][s], uyp = st->up[2][s], unp = st->up[3][s];
+    const double fx = 1 / c->dx / 2, fy = 1 / c->dy / 2, fz = 1 / c->dz / 2;
+    const int sy = st->ncx, sz = st->ncx * st->ncy;
+    const double dxut = (U0[s + 1] - U0[s - 1]) * fx, dxux = (U1[s + 1] - U1[s - 1]) * fx;
+    const double dxuy = (U2[s + 1] - U2[s - 1]) * fx, dxun = (U3[s + 1] - U3[s - 1]) * fx;
+    const double dyut = (U0[s + sy] - U0[s - sy]) * fy, dyux = (U1[s + sy] - U1[s - sy]) * fy;
+    const double dyuy = (U2[s + sy] - U2[s - sy]) * fy, dyun = (U3[s + sy] - U3[s - sy]) * fy;
+    const double dnut = (U0[s + sz] - U0[s - sz]) * fz, dnux = (U1[s + sz] - U1[s - sz]) * fz;
+    const double dnuy = (U2[s + sz] - U2[s - sz]) * fz, dnun = (U3[s + sz] - U3[s - sz]) * fz;
+    const double dtut = (ut - utp) / dt, dtux = (ux - uxp) / dt, dtuy = (uy - uyp) / dt, dtun = (un - unp) / dt;
+
+    const double ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
+    const double Dut = ut * dtut + ux * dxut + uy * dyut + un * dnut + t * un * un;
+    const double dut = Dut - t * un * un;
+    const double dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;
+    const double duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
+    const double dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
+    const double theta = ut / t + dtut + dxux + dyuy + dnun;
+    const double stt = -t * ut * un2 + (dtut - ut * dut) + (ut2 - 1) * theta / 3;
+    const double stx = -(t * un2 * ux) / 2 + (dtux - dxut) / 2 - (ux * dut + ut * dux) / 2 + ut * ux * theta / 3;
+    const double sty = -(t * un2 * uy) / 2 + (dtuy - dyut) / 2 - (uy * dut + ut * duy) / 2 + ut * uy * theta / 3;
+    const double stn = -un * (2 * ut2 + t2 * un2) / (2 * t) + (dtun - dnut / t2) / 2 - (un * dut + ut * dun) / 2 +
+                       ut * un * theta / 3;
+    const double sxx = -(dxux + ux * dux) + (1 + ux * ux) * theta / 3;
+    const double sxy = -(dxuy + dyux) / 2 - (uy * dux + ux * duy) / 2 + ux * uy * theta / 3;
+    const double sxn = -ut * ux * un / t - (dxun + dnux / t2) / 2 - (un * dux + ux * dun) / 2 + ux * un * theta / 3;
+    const double syy = -(dyuy + uy * duy) + (1 + uy * uy) * theta / 3;
+    const double syn = -ut * uy * un / t - (dyun + dnuy / t2) / 2 - (un * duy + uy * dun) / 2 + uy * un * theta / 3;
+    const double snn = -ut * (1 + 2 * t2 * un2) / t3 - dnun / t2 - un * dun + (1 / t2 + un2) * theta / 3;
+
+    const double F = 1 + (ux * ux + uy * uy);
+    const double z0 = t * un / sqrt(F), z3 = ut / t / sqrt(F);
+    const double z02 = z0 * z0, z0z3 = z0 * z3, z32 = z3 * z3;
+    const double A = z02 * stt - 2 * t2 * z0z3 * stn + t2 * t2 * z32 * snn;
+    const double B0 = z0 * stt - t2 * z3 * stn, B1 = z0 * stx - t2 * z3 * sxn;
+    const double B2 = z0 * sty - t2 * z3 * syn, B3 = z0 * stn - t2 * z3 * snn;
+    const double thetaT = 2 * theta / 3 + A;  /* the last of the reference's assignments (:183-184) */
+    const double zDzu = theta - thetaT;
+    const double sttT = stt + 2 * z0 * B0 + z02 * A - 0.5 * (1 - ut * ut + z02) * A;
+    const double stxT = stx + z0 * B1 - 0.5 * (-ut * ux) * A;
+    const double styT = sty + z0 * B2 - 0.5 * (-ut * uy) * A;
+    const double stnT = stn + z0 * B3 + z3 * B0 + z0z3 * A - 0.5 * (-ut * un + z0z3) * A;
+    const double sxxT = sxx - 0.5 * (-1 - ux * ux) * A;
+    const double sxyT = sxy - 0.5 * (-ux * uy) * A;
+    const double sxnT = sxn + z3 * B1 - 0.5 * (-ux * un) * A;
+    const double syyT = syy - 0.5 * (-1 - uy * uy) * A;
+    const double synT = syn + z3 * B2 - 0.5 * (-uy * un) * A;
+    const double snnT = snn + 2 * z3 * B3 + z32 * A - 0.5 * (-1 / t2 - un * un + z32) * A;
+    v[12][s] = stt - sxx - syy - t2 * snn;
+    v[13][s] = sttT - sxxT - syyT - t2 * snnT;
+    v[14][s] = z02 * stt - 2 * t2 * z0z3 * stn + t2 * t2 * z32 * snn;
+    v[15][s] = snnT;
+
+    const double Pi = has_bulk(c) ? qn[SLOT_PI][s] : 0.0;
+    const double cs2 = eos_cs2(c, e_s);
+    const double T = eos_T(c, e_s);
+    const double etabar = c->etabar;
+    v[0][s] = 5 * etabar * fabs(thetaT) / T;
+    v[1][s] = 5 * etabar * fabs(zDzu) / T;
+    v[2][s] = 5 * etabar * fabs(theta) / T;
+    double pl = 0, ptHat = 0, ps = 0, ap[16];
+    if (has_pimunu(c)) {
+        pl = qn[SLOT_PL][s];
+        const double pitt = qn[5][s], pitx = qn[6][s], pity = qn[7][s], pitn = qn[8][s], pixx = qn[9][s];
+        const double pixy = qn[10][s], pixn = qn[11][s], piyy = qn[12][s], piyn = qn[13][s], pinn = qn[14][s];
+        const double pipi = pitt * pitt - 2 * pitx * pitx - 2 * pity * pity + pixx * pixx + 2 * pixy * pixy +
+                            piyy * piyy - 2 * pitn * pitn * t2 + 2 * pixn * pixn * t2 + 2 * piyn * piyn * t2 +
+                            pinn * pinn * t2 * t2;
+        ptHat = pt_hat(e_s, p_s, pl);
+        v[4][s] = sqrt(fabs(pipi)) / fabs(ptHat);
+    }
+    if (has_bulk(c)) {
+        const double b = 0.333333 - cs2;
+        const double tauPiInv = 15 * (b * b) * T / zeta_over_s(c, T);
+        v[3][s] = fabs(thetaT + zDzu) / tauPiInv;
+        v[5][s] = fabs(Pi) / fabs(ptHat);
+    }
+    v[8][s] = 5 * etabar / T;
+    v[9][s] = dxux;
+    v[10][s] = dyuy;
+    v[11][s] = thetaT + zDzu;
+    if (has_pimunu(c)) {
+        powers(pl / e_s, ap);
+        const double Rtilde = VO_RATIO(Rtilde, ap), Rhat = VO_RATIO(Rhat, ap);
+        const double Rbar0 = VO_RATIO(Rbar0, ap), Rgamma = VO_RATIO(Rgamma, ap);
+        const second_order so = second_order_z(e_s, p_s, pl, cs2, ap);
+        const double etaBar_TC = ((3 - Rtilde) * e_s - 2 * pl) / 8;
+        const double delta_pipi = (3 + Rgamma) / 2;
+        const double tau_pipi = 4 * (delta_pipi - 0) / 3;  /* :294, 1/2 -> 0 */
+        const double lambda_pipi = Rgamma - 1;
+        const double pi[10] = {qn[5][s], qn[6][s], qn[7][s], qn[8][s], qn[9][s],
+                               qn[10][s], qn[11][s], qn[12][s], qn[13][s], qn[14][s]};
+        const double pitt = pi[0], pitx = pi[1], pity = pi[2], pitn = pi[3], pixx = pi[4];
+        const double pixy = pi[5], pixn = pi[6], piyy = pi[7], piyn = pi[8], pinn = pi[9];
+        ps = pitt * sttT - 2 * pitx * stxT - 2 * pity * styT + pixx * sxxT + 2 * pixy * sxyT + piyy * syyT -
+             2 * pitn * stnT * t2 + 2 * pixn * sxnT * t2 + 2 * piyn * synT * t2 + pinn * snnT * t2 * t2;
+        const double ps2 = ps / 2;
+        const double I4[10] = {
+            (pitt * sttT - pitx * stxT - pity * styT - t2 * pitn * stnT) - (1 - ut2 + z02) * ps2,
+            (pitt * stxT + pitx * sttT) / 2 - (pitx * sxxT + pixx * stxT) / 2 - (pity * sxyT + pixy * styT) / 2 -
+                t2 * (pitn * sxnT + pixn * stnT) / 2 + (ut * ux) * ps2,
+            (pitt * styT + pity * sttT) / 2 - (pitx * sxyT + pixy * stxT) / 2 - (pity * syyT + piyy * styT) / 2 -
+                t2 * (pitn * synT + piyn * stnT) / 2 + (ut * uy) * ps2,
+            (pitt * stnT + pitn * sttT) / 2 - (pitx * sxnT + pixn * stxT) / 2 - (pity * synT + piyn * styT) / 2 -
+                t2 * (pitn * snnT + pinn * stnT) / 2 + (ut * un - z0z3) * ps2,
+            (pitx * stxT - pixx * sxxT - pixy * sxyT - t2 * pixn * sxnT) + (1 + ux * ux) * ps2,
+            (pitx * styT + pity * stxT) / 2 - (pixx * sxyT + pixy * sxxT) / 2 - (pixy * syyT + piyy * sxyT) / 2 -
+                t2 * (pixn * synT + piyn * sxnT) / 2 + (ux * uy) * ps2,
+            (pitx * stnT + pitn * stxT) / 2 - (pixx * sxnT + pixn * sxxT) / 2 - (pixy * synT + piyn * sxyT) / 2 -
+                t2 * (pixn * snnT + pinn * sxnT) / 2 + (ux * un) * ps2,
+            (pity * styT - pixy * sxyT - piyy * syyT - t2 * piyn * synT) + (1 + uy * uy) * ps2,
+            (pity * stnT + pitn * styT) / 2 - (pixy * sxnT + pixn * sxyT) / 2 - (piyy * synT + piyn * syyT) / 2 -
+                t2 * (piyn * snnT + pinn * synT) / 2 + (uy * un) * ps2,
+            (pitn * stnT - pixn * sxnT - piyn * synT - t2 * pinn * snnT) + (1 / t2 + un2 - z32) * ps2};
+        /* J = delta I2 + tau I4 - lambda I5 - lambda_piPi Pi sigma^{tt}_T in every component (:335-344) */
+        double J[10];
+        for (int m = 0; m < 10; ++m)
+            J[m] = delta_pipi * (thetaT * pi[m]) + tau_pipi * I4[m] - lambda_pipi * (zDzu * pi[m]) -
+                   so.lambda_piPi * Pi * sttT;
+        const double ss = sttT * sttT - 2 * stxT * stxT - 2 * styT * styT + sxxT * sxxT + 2 * sxyT * sxyT +
+                          syyT * syyT - 2 * stnT * stnT * t2 + 2 * sxnT * sxnT * t2 + 2 * synT * synT * t2 +
+                          snnT * snnT * t2 * t2;
+        const double JJ = J[0] * J[0] - 2 * J[1] * J[1] - 2 * J[2] * J[2] + J[4] * J[4] + 2 * J[5] * J[5] +
+                          J[7] * J[7] - 2 * J[3] * J[3] * t2 + 2 * J[6] * J[6] * t2 + 2 * J[8] * J[8] * t2 +
+                          J[9] * J[9] * t2 * t2;
+        v[6][s] = sqrt(fabs(JJ / ss)) / 2 / etaBar_TC;
+        if (has_bulk(c)) {
+            const double zeta_z = (Rhat - Rbar0) * (e_s - 3 * p_s) / 3;
+            const double zeta_T = -(Rbar0 + Rhat) * (e_s - 3 * p_s) / 6;
+            const double Jb = -so.beta_PiPi * Pi * zDzu - so.delta_PiPi * Pi * thetaT + so.lambda_Pipi * ps;
+            v[7][s] = (double)fabsf((float)(Jb / (-zeta_z * zDzu - zeta_T * thetaT)));  /* :391, fabsf */
+        }
+    }
+}
+
+static void check_validity(vo_state *st, double t, double dt, double *const *qn) {
+    for (int i = 2; i < st->ncx - 2; ++i)
+        for (int j = 2; j < st->ncy - 2; ++j)
+            for (int k = 2; k < st->ncz - 2; ++k) validity_cell(st, t, dt, qn, idx(st, i, j, k));
+}
+
+void vo_set_validity(vo_state *st, int on) {
+    if (on && !st->vd[0])
+        for (int m = 0; m < VO_NUM_VALIDITY; ++m) st->vd[m] = (double *)calloc(st->len, sizeof(double));
+    st->validity_on = on && st->vd[0] != NULL;
+}
+
+double *vo_validity_field(vo_state *st, int id) {
+    return (id >= 0 && id < VO_NUM_VALIDITY) ? st->vd[id] : NULL;
 }
 
 /* DynamicalVariables.cpp:349-489: zero-gradient ghost layers, I then J then
@@ -751,6 +923,7 @@ void vo_step(vo_state *st, double t, double dt) {
     infer_all(st, t, st->Q, st->up, st->u);
     regulate(st, t, st->Q, st->u);
     ghosts(st, st->Q, st->u);
+    if (st->validity_on) check_validity(st, t, dt, st->q);  /* :791, before q and Q swap */
 
     for (int n = 0; n < NQ_MAX; ++n) {
         double *tmp = st->q[n];
@@ -839,6 +1012,7 @@ void vo_destroy(vo_state *st) {
     for (int n = 0; n < NQ_MAX; ++n) { free(st->q[n]); free(st->Q[n]); free(st->qS[n]); }
     free(st->e); free(st->p);
     for (int m = 0; m < 4; ++m) { free(st->u[m]); free(st->up[m]); free(st->uS[m]); }
+    for (int m = 0; m < VO_NUM_VALIDITY; ++m) free(st->vd[m]);
     free(st);
 }
 

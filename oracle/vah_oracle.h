@@ -50,6 +50,14 @@ double vo_run(vo_state *st, double t0, double dt, int nsteps);
  * out[0] face (flux) fallbacks, out[1] cell fallbacks, out[2] NaNs */
 void vo_last_step_stats(const vo_state *st, long long out[3]);
 
+/* Validity diagnostics (HydrodynamicValidity.cpp:47-394, computed at the end
+ * of every step, FullyDiscreteKurganovTadmorScheme.cpp:791) and the regulator
+ * maps (same file :652-693), in the order of include/vah.h's VAH_V_* ids.
+ * Off until vo_set_validity(st, 1); arrays are ncx*ncy*ncz, interior written. */
+#define VO_NUM_VALIDITY 27
+void vo_set_validity(vo_state *st, int on);
+double *vo_validity_field(vo_state *st, int id);
+
 /* Single-cell operators, for unit tests of the library's pieces. */
 int vo_infer(const vo_config *cfg, double t, const double *q, double ePrev, double uT0,
              double *out /* e, p, ut, ux, uy, un */);

@@ -129,3 +129,33 @@ def test_limiter_matches_minmod_definition():
 
         assert L.vo_approx_derivative(a, b, c) == mm(l, mm(cc, r))
     assert L.vo_approx_derivative(1.0, 1.0, 1.0) == 0.0
+
+
+@pytest.mark.parametrize("physics,eos,shape", [("pimunu", "conformal", (9, 8, 5)), ("pimunu_pi", "table", (9, 8, 5)),
+                                               ("pimunu", "table", (11, 9, 1))])
+def test_validity_diagnostics_match_the_reference_bit_for_bit(physics, eos, shape):
+    """The oracle's restatement of the validity diagnostics and regulator maps
+    against the reference's own VALIDITY_DOMAIN arrays after three steps."""
+    if not V.ref_available(V.PHYSICS[physics], {"conformal": 0, "table": 1}[eos]):
+        pytest.skip("reference build not present")
+    tab = V.eos_table() if eos == "table" else None
+    g = V.Grid(*shape, 0.2, 0.2, 0.2, 0.2, physics=physics, eos=eos,
+               zeta="crossover" if eos == "table" else "reference", table=tab)
+    o, r = V.Oracle(g), V.Reference(g)
+    o.set_validity(1)
+    f = V.smooth_initial_state(g, 0.5, pi_amp=0.3)
+    V.load_state(o, f)
+    V.load_state(r, f)
+    o.set_conserved(0.5, 0)
+    r.set_conserved(0.5)
+    o.set_ghost_cells()
+    r.set_ghost_cells()
+    for n in range(3):
+        o.step(0.5 + 0.02 * n, 0.02)
+        r.step(0.5 + 0.02 * n, 0.02)
+    nonzero = 0
+    for vid in range(V.NUM_VALIDITY):
+        a, b = g.interior(o.validity(vid)), g.interior(r.validity(vid))
+        np.testing.assert_array_equal(a, b, err_msg=f"validity field {vid}")
+        nonzero += bool(np.any(b != 0))
+    assert nonzero >= (27 if physics == "pimunu_pi" else 24)

@@ -68,6 +68,9 @@ def oracle_lib():
         L.vo_approx_derivative.argtypes = [D, D, D]
         L.vo_approx_derivative.restype = D
         L.vo_eos_eval.argtypes = [C.POINTER(VOConfig), D, P]
+        L.vo_set_validity.argtypes = [C.c_void_p, I]
+        L.vo_validity_field.restype = P
+        L.vo_validity_field.argtypes = [C.c_void_p, I]
         _oracle = L
     return _oracle
 
@@ -134,8 +137,23 @@ class Oracle:
         self.L.vo_last_step_stats(self.st, out)
         return list(out)
 
+    def set_validity(self, on):
+        self.L.vo_set_validity(self.st, int(on))
+
+    def validity(self, vid):
+        return np.ctypeslib.as_array(self.L.vo_validity_field(self.st, vid), (self.g.ncell,))
+
 
 # ---------------------------------------------------- the reference itself --
+# Validity ids (include/vah.h VAH_V_*) -> member index in the reference's
+# VALIDITY_DOMAIN (DynamicalVariables.h:86-117): knTaupiT, knTaupiL, knTaupi,
+# knTauPi, Rpi, RPi, Rpi2, RPi2, taupi, dxux, dyuy, theta, stt, sxx, syy, snn,
+# regulations, regMag, regTr, regU0-3, regZ0-3.
+REF_VALIDITY_MEMBER = [0, 1, 2, 3, 4, 5, 7, 8, 26, 27, 28, 29, 22, 23, 24, 25, 11, 12, 13, 14, 15, 16, 17, 18, 19,
+                       20, 21]
+NUM_VALIDITY = 27
+
+
 def ref_path(physics, eos):
     name = {0: "ideal", 1: "pimunu", 2: "pimunu_pi"}[physics]
     return os.path.join(ROOT, "oracle", "_ref", f"libvahref_{name}_{'conf' if eos == 0 else 'table'}.so")
@@ -173,6 +191,13 @@ class Reference:
 
     def field(self, fid):
         p = self.L.vref_field(fid)
+        return np.ctypeslib.as_array(p, (self.g.ncell,)) if p else None
+
+    def validity(self, vid):
+        """The reference's own VALIDITY_DOMAIN array for a VAH_V_* id."""
+        self.L.vref_validity.restype = P
+        self.L.vref_validity.argtypes = [I]
+        p = self.L.vref_validity(REF_VALIDITY_MEMBER[vid])
         return np.ctypeslib.as_array(p, (self.g.ncell,)) if p else None
 
     def set_conserved(self, t):
