@@ -18,6 +18,7 @@
 
 using vah::FieldSet;
 using vah::StageArgs;
+using vah::ValidityArgs;
 
 struct vah_event {
     vah_lattice lat;
@@ -42,6 +43,9 @@ struct vah_event {
     long long steps;
     double last_t, last_dt;          // time and step of the latest vah_rk2_step (autotuning state)
     double *d_stage64;               // FP32 storage: one FP64 field of staging for the host-buffer step
+    bool validity;                   // fill the validity diagnostics every step
+    double *vd[VAH_NUM_VALIDITY];    // validity fields (FP64, ghosted layout)
+    void *vq[16];                    // P_L, pi, Pi at the start of the step (validity input)
     vah::SplitConfig split;          // launch configuration of the face/cell kernels
     bool timing;
     std::vector<cudaEvent_t> tev;  // start/stop pairs of timed launches
@@ -100,6 +104,8 @@ void free_all(vah_event *ev) {
     cudaFree(ev->d_exc);
     cudaFree(ev->d_counters);
     cudaFree(ev->d_stage64);
+    for (int m = 0; m < VAH_NUM_VALIDITY; ++m) cudaFree(ev->vd[m]);
+    for (int n = 0; n < 16; ++n) cudaFree(ev->vq[n]);
     for (cudaEvent_t e : ev->tev) cudaEventDestroy(e);
     if (ev->own_stream && ev->stream) cudaStreamDestroy(ev->stream);
 }
@@ -134,6 +140,8 @@ void fill_common(const vah_event *ev, StageArgs<S> &a) {
             a.H[d][n] = (S *)ev->H[d][n];
             a.HR[d][n] = (S *)ev->HR[d][n];
         }
+    if (ev->validity)
+        for (int m = 0; m < 11; ++m) a.regmap[m] = ev->vd[VAH_V_REGULATIONS + m];
 }
 
 template <typename S>
@@ -201,6 +209,9 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->steps = 0;
     ev->last_t = hydro->t0;
     ev->d_stage64 = nullptr;
+    ev->validity = false;
+    memset(ev->vd, 0, sizeof(ev->vd));
+    memset(ev->vq, 0, sizeof(ev->vq));
     ev->last_dt = 0.005;
     ev->split = vah::default_split_config();
     ev->nexc = 0;
@@ -427,6 +438,9 @@ void stage1_args(const vah_event *ev, double t, double dt, StageArgs<S> &a) {
 template <typename S>
 int rk2_step_t(vah_event *ev, double t, double dt) {
     const int c = ev->cur, o = 1 - ev->cur;
+    if (ev->validity)  // the diagnostics read P_L, pi, Pi as they are at the start of the step
+        for (int n = VAH_F_PL; n < ev->nq; ++n)
+            VAH_TRY(cudaMemcpyAsync(ev->vq[n], ev->q[n], ev->ncell * sizeof(S), cudaMemcpyDeviceToDevice, ev->stream));
     StageArgs<S> a;
     stage1_args(ev, t, dt, a);
     int rc = timed_launch(ev, a);
@@ -453,7 +467,32 @@ int rk2_step_t(vah_event *ev, double t, double dt) {
     a.pin = (const S *)ev->ep[o][1];
     a.eout = (S *)ev->ep[c][0];
     a.pout = (S *)ev->ep[c][1];
-    return timed_launch(ev, a);
+    rc = timed_launch(ev, a);
+    if (rc != VAH_OK || !ev->validity) return rc;
+    ValidityArgs<S> v;
+    memset(&v, 0, sizeof(v));
+    v.nx = ev->lat.nx;
+    v.ny = ev->lat.ny;
+    v.nz = ev->lat.nz;
+    v.ncx = ev->ncx;
+    v.ncy = ev->ncy;
+    v.plane = (long long)ev->ncx * ev->ncy;
+    v.t = t + dt;
+    v.dt = dt;
+    v.dx = ev->lat.dx;
+    v.dy = ev->lat.dy;
+    v.dz = ev->lat.dz;
+    v.etabar = ev->hydro.eta_over_s;
+    for (int n = 0; n < 16; ++n) v.qn[n] = (const S *)ev->vq[n];
+    v.e = (const S *)ev->ep[c][0];
+    v.p = (const S *)ev->ep[c][1];
+    for (int m = 0; m < 4; ++m) {
+        v.u[m] = (const S *)ev->up[m];  // the new velocity (the buffers swap after this call)
+        v.up[m] = (const S *)ev->u[m];
+    }
+    v.eos = make_eos(ev);
+    for (int m = 0; m < 16; ++m) v.v[m] = ev->vd[m];
+    return cuda_status(vah::launch_validity<S>(v, ev->opt.physics, ev->stream));
 }
 
 }  // namespace
@@ -545,6 +584,43 @@ extern "C" int vah_event_autotune(vah_event *ev, int reps, vah_tune_report *out)
     if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED) return VAH_OK;  // one fused launch shape: nothing to tune
     VAH_TRY(cudaSetDevice(ev->opt.device));
     return ev->elem == sizeof(float) ? autotune_t<float>(ev, reps, out) : autotune_t<double>(ev, reps, out);
+}
+
+extern "C" int vah_event_set_validity(vah_event *ev, int on) {
+    if (!ev) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(ev->opt.device));
+    if (on && !ev->vd[0]) {
+        for (int m = 0; m < VAH_NUM_VALIDITY; ++m) {
+            cudaError_t e = cudaMalloc((void **)&ev->vd[m], ev->ncell * sizeof(double));
+            if (e == cudaSuccess) e = cudaMemsetAsync(ev->vd[m], 0, ev->ncell * sizeof(double), ev->stream);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        for (int n = VAH_F_PL; n < ev->nq; ++n) {
+            cudaError_t e = cudaMalloc(&ev->vq[n], ev->ncell * ev->elem);
+            if (e == cudaSuccess) e = cudaMemsetAsync(ev->vq[n], 0, ev->ncell * ev->elem, ev->stream);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+    }
+    ev->validity = on != 0;
+    return VAH_OK;
+}
+
+extern "C" int vah_event_get_validity(vah_event *ev, int id, double *host, int with_ghosts) {
+    if (!ev || !host || id < 0 || id >= VAH_NUM_VALIDITY || !ev->vd[id]) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(ev->opt.device));
+    VAH_TRY(cudaStreamSynchronize(ev->stream));
+    const size_t es = sizeof(double);
+    if (with_ghosts) {
+        VAH_TRY(cudaMemcpy(host, ev->vd[id], ev->ncell * es, cudaMemcpyDeviceToHost));
+        return VAH_OK;
+    }
+    const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz;
+    for (int k = 0; k < nz; ++k) {
+        const double *row = ev->vd[id] + 2 + (size_t)ev->ncx * (2 + (size_t)ev->ncy * (k + 2));
+        VAH_TRY(cudaMemcpy2D(host + (size_t)nx * ny * k, nx * es, row, ev->ncx * es, nx * es, ny,
+                             cudaMemcpyDeviceToHost));
+    }
+    return VAH_OK;
 }
 
 extern "C" int vah_run(vah_event *ev, double t0, double dt, int nsteps) {

@@ -75,6 +75,7 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
     a.eos = eos;
     a.counters = d.counters;
     a.fallback = d.fallback;
+    for (int m = 0; m < 11; ++m) a.regmap[m] = nullptr;  // validity diagnostics are an event-path option
     a.hot = d.hot;
     a.e_freeze = d.e_freeze;
     a.crossings = d.crossings;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "vah_stage.cuh"
+#include "vah_validity.cuh"
 
 namespace vah {
 
@@ -72,6 +73,10 @@ cudaError_t launch_stage_split(const StageArgs<S> &a, int physics, bool exact, c
                                cudaStream_t stream);
 template <typename S>
 cudaError_t launch_stage_split(const StageArgs<S> &a, int physics, bool exact, cudaStream_t stream);
+
+// Validity diagnostics of every interior cell after a step.
+template <typename S>
+cudaError_t launch_validity(const ValidityArgs<S> &a, int physics, cudaStream_t stream);
 
 // A set of device field pointers, passed to kernels by value.
 template <typename S>

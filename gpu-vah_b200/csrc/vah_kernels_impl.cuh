@@ -62,6 +62,15 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) cell_kernel(const StageAr
 }
 
 template <typename S, int PHYS>
+__global__ void validity_kernel(const ValidityArgs<S> a) {
+    const long long n = (long long)a.nx * a.ny * a.nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % a.nx), j = (int)((c / a.nx) % a.ny), k = (int)(c / ((long long)a.nx * a.ny));
+        validity_cell<S, PHYS>(a, (i + 2) + (long long)a.ncx * (j + 2) + a.plane * (k + 2));
+    }
+}
+
+template <typename S, int PHYS>
 __global__ void set_conserved_kernel(const FieldSet<S> q, const FieldSet<S> u, const FieldSet<S> up, const S *e,
                                      int nx, int ny, int nz, double t, int pl_from_field) {
     const long long n = (long long)nx * ny * nz;
@@ -225,6 +234,18 @@ cudaError_t launch_stage_split(const StageArgs<S> &a, int physics, bool exact, c
 }
 
 template <typename S>
+cudaError_t launch_validity(const ValidityArgs<S> &a, int physics, cudaStream_t stream) {
+    const int block = 128, grid = grid_for((long long)a.nx * a.ny * a.nz, block);
+    switch (physics) {
+    case kIdeal: validity_kernel<S, kIdeal><<<grid, block, 0, stream>>>(a); break;
+    case kPimunu: validity_kernel<S, kPimunu><<<grid, block, 0, stream>>>(a); break;
+    case kPimunuPi: validity_kernel<S, kPimunuPi><<<grid, block, 0, stream>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename S>
 cudaError_t launch_set_conserved(const FieldSet<S> &q, const FieldSet<S> &u, const FieldSet<S> &up, const S *e,
                                  int physics, int nx, int ny, int nz, double t, int pl_from_field,
                                  cudaStream_t stream) {
@@ -266,6 +287,7 @@ cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cud
 
 #define VAH_INSTANTIATE(S)                                                                                      \
     template cudaError_t launch_stage<S>(const StageArgs<S> &, int, cudaStream_t);                              \
+    template cudaError_t launch_validity<S>(const ValidityArgs<S> &, int, cudaStream_t);                        \
     template cudaError_t launch_split_kind<S>(const StageArgs<S> &, int, bool, int, const KindConfig &,         \
                                               cudaStream_t);                                                    \
     template cudaError_t launch_stage_split<S>(const StageArgs<S> &, int, bool, const SplitConfig &,            \

@@ -646,8 +646,11 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, doub
 // -------------------------------------------------------------- regulator --
 // FullyDiscreteKurganovTadmorScheme.cpp:524-696: e < 0 -> e = p = 1e-7,
 // P_L < 0 -> 1e-7, then pi^{mu nu} *= tanh(rho)/rho (xi0 = rho_max = 1).
+// maps (optional, 11 values, written only with shear): the applied factor and
+// each criterion's own factor tanh(a)/a (1 below 1e-7) in the order
+// magnitude, trace, u-orthogonality x4, z-orthogonality x4 (:666-693).
 template <int PHYS>
-VAH_HD void regulate(double t, double &e, double &p, double *q, const double *u) {
+VAH_HD void regulate(double t, double &e, double &p, double *q, const double *u, double *maps = nullptr) {
     if (e < 0.0) {
         e = 1.e-7;
         p = 1.e-7;
@@ -690,6 +693,12 @@ VAH_HD void regulate(double t, double &e, double &p, double *q, const double *u)
     if (rho < 1.e-7) fac = 1.0;
 #pragma unroll
     for (int n = 5; n < 15; ++n) q[n] *= fac;
+    if (maps) {
+        const double a1 = spipi / sTrsTrs;
+        maps[0] = fac;
+        maps[1] = a1 < 1.e-7 ? 1.0 : tanh(a1) / a1;
+        for (int m = 0; m < 9; ++m) maps[2 + m] = cand[m] < 1.e-7 ? 1.0 : tanh(cand[m]) / cand[m];
+    }
 }
 
 }  // namespace vah

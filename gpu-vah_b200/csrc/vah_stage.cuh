@@ -38,6 +38,7 @@ struct StageArgs {
     Eos eos;
     unsigned long long *counters;  // [face fallbacks, cell fallbacks, NaN cells]
     unsigned char *fallback;       // optional: per ghosted cell, 1 where this stage's inversion fell back
+    double *regmap[11];            // optional (validity diagnostics): the regulator's factors per ghosted cell
     // optional freeze-out crossing test at the end of a step (stage 2): per
     // ghosted cell 1 while e > e_freeze; crossings counted [down, up]
     unsigned char *hot;
@@ -186,7 +187,10 @@ VAH_HD void stage_cell(const StageArgs<S> &a, int i, int j, int k) {
     const int st = invert<PHYS>(a.eos, a.t_inv, qfull, g.e, sqrt(fabs(gx * gx + gy * gy)), prim);
     double e = prim[0], p = prim[1];
     double u[4] = {prim[2], prim[3], prim[4], prim[5]};
-    regulate<PHYS>(a.t_inv, e, p, val, u);
+    double rmap[11];
+    regulate<PHYS>(a.t_inv, e, p, val, u, a.regmap[0] ? rmap : nullptr);
+    if (a.regmap[0] && Phys<PHYS>::PIMUNU)
+        for (int m = 0; m < 11; ++m) a.regmap[m][s] = rmap[m];
 
     if ((fails & 255u) && a.counters) count_add(a.counters + 0, fails & 255u);
     if (st != 0 && a.counters) count_add(a.counters + 1, 1ull);
@@ -292,7 +296,10 @@ VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
     const int st = invert<PHYS>(a.eos, a.t_inv, qfull, g.e, sqrt(fabs(gx * gx + gy * gy)), prim);
     double e = prim[0], p = prim[1];
     double u[4] = {prim[2], prim[3], prim[4], prim[5]};
-    regulate<PHYS>(a.t_inv, e, p, val, u);
+    double rmap[11];
+    regulate<PHYS>(a.t_inv, e, p, val, u, a.regmap[0] ? rmap : nullptr);
+    if (a.regmap[0] && Phys<PHYS>::PIMUNU)
+        for (int m = 0; m < 11; ++m) a.regmap[m][s] = rmap[m];
     if (st != 0 && a.counters) count_add(a.counters + 1, 1ull);
     if ((bad || st == 2) && a.counters) count_add(a.counters + 2, 1ull);
     if (a.fallback) a.fallback[s] = st != 0;

@@ -23,6 +23,10 @@ VAH_PL_REFERENCE, VAH_PL_ISOTROPIC = 0, 1
 NUM_FIELDS = 26
 F_E, F_P, F_UT, F_UX, F_UY, F_UN = 16, 17, 18, 19, 20, 21
 HBARC = 0.197326938
+NUM_VALIDITY = 27  # VAH_NUM_VALIDITY
+VALIDITY_NAMES = ["knTaupiT", "knTaupiL", "knTaupi", "knTauPi", "Rpi", "RPi", "Rpi2", "RPi2", "taupi", "dxux", "dyuy",
+                  "theta", "stt", "sxx", "syy", "snn", "regulations", "regMag", "regTr", "regU0", "regU1", "regU2",
+                  "regU3", "regZ0", "regZ1", "regZ2", "regZ3"]
 
 STATUS = {0: "VAH_OK", -1: "VAH_ERR_ARG", -2: "VAH_ERR_CUDA", -3: "VAH_ERR_NOMEM", -4: "VAH_ERR_NAN",
           -5: "VAH_ERR_NODEVICE", -6: "VAH_ERR_TOO_LARGE"}
@@ -75,7 +79,8 @@ EXPORTS = ["vah_version", "vah_eos_table_build", "vah_event_create", "vah_event_
            "vah_rk2_step", "vah_run", "vah_event_sync", "vah_event_stats", "vah_event_set_timing",
            "vah_event_kernel_time", "vah_rk2_step_host", "vah_ic_optical_glauber", "vah_ic_mc_glauber",
            "vah_ic_longitudinal", "vah_event_autotune", "vah_batch_autotune",
-           "vah_batch_freezeout_volume", "vah_batch_fallback_mask"]
+           "vah_batch_freezeout_volume", "vah_batch_fallback_mask", "vah_event_set_validity",
+           "vah_event_get_validity"]
 
 _lib = None
 
@@ -228,6 +233,16 @@ class Event:
         ms, n = D(), C.c_longlong()
         check(self.L.vah_event_kernel_time(self.ev, C.byref(ms), C.byref(n)), "vah_event_kernel_time")
         return ms.value, n.value
+
+    def set_validity(self, on):
+        """Fill the validity diagnostics (VAH_V_* fields) at every following step."""
+        check(self.L.vah_event_set_validity(self.ev, int(on)), "vah_event_set_validity")
+
+    def get_validity(self, vid, with_ghosts=True):
+        out = np.empty(self.ncell if with_ghosts else self.nx * self.ny * self.nz)
+        check(self.L.vah_event_get_validity(self.ev, vid, out.ctypes.data_as(P), int(with_ghosts)),
+              "vah_event_get_validity")
+        return out
 
     def autotune(self, reps=3):
         """Pick the fastest launch configuration per kernel kind (vah_event_autotune); returns the choices."""

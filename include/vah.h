@@ -189,6 +189,44 @@ int vah_event_stats(vah_event *ev, vah_stats *out);
 int vah_event_set_timing(vah_event *ev, int on);
 int vah_event_kernel_time(vah_event *ev, double *ms, long long *launches);
 
+/* ---- validity diagnostics (HydrodynamicValidity.cpp:47-394) ----
+ * The reference computes these at the end of every step
+ * (FullyDiscreteKurganovTadmorScheme.cpp:791) from the conserved state at the
+ * start of the step, the new e, p, u and the previous u, and the regulator
+ * stores its factors (:652-693); nothing in the step reads them, and its
+ * outputs of them are commented out (HydroPlugin.cpp:48-105). Here they are
+ * off by default. vah_event_set_validity(ev, 1) allocates 27 FP64 fields (and
+ * a copy of P_L, pi, Pi taken at the start of each step) and makes every
+ * following vah_rk2_step fill them: the regulator maps from the stage-2 cell
+ * launch, the rest from one launch after it. Interior cells only; ghost cells
+ * read 0. Ids, with the reference's file names in brackets: */
+enum {
+    VAH_V_KN_TAUPI_T = 0,  /* knudsenNumberTaupiT [knTaupiT]: 5 etabar |theta_T| / T */
+    VAH_V_KN_TAUPI_L = 1,  /* knudsenNumberTaupiL [knTaupiL]: 5 etabar |z.D.u| / T */
+    VAH_V_KN_TAUPI = 2,    /* knudsenNumberTaupi [knTaupi] */
+    VAH_V_KN_TAUPI_BULK = 3, /* knudsenNumberTauPi [knTauPi] (shear + bulk) */
+    VAH_V_RPI = 4,         /* Rpi [Rpi]: sqrt|pi.pi| / |P_T hat| */
+    VAH_V_RPI_BULK = 5,    /* RPi [RPi]: |Pi| / |P_T hat| (shear + bulk) */
+    VAH_V_RPI2 = 6,        /* Rpi2 [Rpi2]: second-order inverse Reynolds number */
+    VAH_V_RPI2_BULK = 7,   /* RPi2 [RPi2] (shear + bulk) */
+    VAH_V_TAUPI = 8,       /* taupi [taupi] = 5 etabar / T */
+    VAH_V_DXUX = 9,        /* dxux [dxux] */
+    VAH_V_DYUY = 10,       /* dyuy [dyuy] */
+    VAH_V_THETA = 11,      /* theta [theta] = theta_T + z.D.u */
+    VAH_V_STT = 12,        /* stt [stt]: the combinations the reference stores last (:197-200) */
+    VAH_V_SXX = 13,        /* sxx [sxx] */
+    VAH_V_SYY = 14,        /* syy [syy] */
+    VAH_V_SNN = 15,        /* snn [snn] */
+    VAH_V_REGULATIONS = 16, /* regulations [regulations]: the factor tanh(rho)/rho applied to pi */
+    VAH_V_REG_MAG = 17,    /* regMag, regTr, regU0..regU3, regZ0..regZ3: each criterion's own factor */
+    VAH_V_REG_TR = 18,
+    VAH_V_REG_U0 = 19,
+    VAH_V_REG_Z0 = 23,
+    VAH_NUM_VALIDITY = 27
+};
+int vah_event_set_validity(vah_event *ev, int on);
+int vah_event_get_validity(vah_event *ev, int id, double *host, int with_ghosts);
+
 /* ---- launch autotuning (no reference counterpart) ----
  * The face/cell kernels come in register-cap variants and take their block
  * shape at run time. vah_event_autotune times every candidate of each launch

@@ -11,6 +11,7 @@
 #include "vah.h"
 #include "vah_powf_exc.h"
 #include "vah_stage.cuh"
+#include "vah_validity.cuh"
 
 namespace {
 
@@ -27,6 +28,8 @@ struct HostEvent {
     vah::Eos eos;
     std::vector<double> tab;
     unsigned long long counters[4];
+    bool validity = false;
+    std::vector<double> vstore, vqstore;  // 27 validity fields; P_L, pi, Pi at the start of the step
 };
 
 template <int PHYS>
@@ -88,6 +91,19 @@ void common(HostEvent *h, vah::StageArgs<double> &a) {
             a.H[d][n] = h->H[d][n];
             a.HR[d][n] = h->HR[d][n];
         }
+}
+
+void set_regmap(HostEvent *h, vah::StageArgs<double> &a) {
+    if (h->validity)
+        for (int m = 0; m < 11; ++m) a.regmap[m] = h->vstore.data() + h->ncell * (VAH_V_REGULATIONS + m);
+}
+
+template <int PHYS>
+void run_validity(const vah::ValidityArgs<double> &v) {
+    for (int k = 0; k < v.nz; ++k)
+        for (int j = 0; j < v.ny; ++j)
+            for (int i = 0; i < v.nx; ++i)
+                vah::validity_cell<double, PHYS>(v, (i + 2) + (long long)v.ncx * (j + 2) + v.plane * (k + 2));
 }
 
 }  // namespace
@@ -162,22 +178,56 @@ void hc_set_conserved(void *p, double t, int pl_from_field) {
             }
 }
 
+void hc_set_validity(void *p, int on) {
+    HostEvent *h = (HostEvent *)p;
+    if (on && h->vstore.empty()) {
+        h->vstore.assign(h->ncell * VAH_NUM_VALIDITY, 0.0);
+        h->vqstore.assign(h->ncell * 16, 0.0);
+    }
+    h->validity = on != 0;
+}
+
+double *hc_validity_field(void *p, int id) {
+    HostEvent *h = (HostEvent *)p;
+    return h->vstore.empty() ? nullptr : h->vstore.data() + h->ncell * id;
+}
+
 void hc_step(void *p, double t, double dt) {
     HostEvent *h = (HostEvent *)p;
     const int c = h->cur, o = 1 - c;
+    if (h->validity)
+        for (int n = 4; n < h->nq; ++n)
+            std::memcpy(h->vqstore.data() + h->ncell * n, h->q[n], h->ncell * sizeof(double));
     vah::StageArgs<double> a;
     common(h, a);
+    set_regmap(h, a);
     a.t_src = t; a.t_inv = t + dt; a.dt = dt; a.stage2 = 0;
     for (int n = 0; n < 16; ++n) { a.qin[n] = h->q[n]; a.qout[n] = h->qS[n]; }
     for (int m = 0; m < 4; ++m) { a.uin[m] = h->u[m]; a.upin[m] = h->up[m]; a.guess[m] = h->u[m]; a.uout[m] = h->uS[m]; }
     a.ein = h->ep[c][0]; a.pin = h->ep[c][1]; a.eout = h->ep[o][0]; a.pout = h->ep[o][1];
     stage(h, a);
     common(h, a);
+    set_regmap(h, a);
     a.t_src = t + dt; a.t_inv = t + dt; a.dt = dt; a.stage2 = 1;
     for (int n = 0; n < 16; ++n) { a.qin[n] = h->qS[n]; a.qavg[n] = h->q[n]; a.qout[n] = h->q[n]; }
     for (int m = 0; m < 4; ++m) { a.uin[m] = h->uS[m]; a.upin[m] = h->u[m]; a.guess[m] = h->u[m]; a.uout[m] = h->up[m]; }
     a.ein = h->ep[o][0]; a.pin = h->ep[o][1]; a.eout = h->ep[c][0]; a.pout = h->ep[c][1];
     stage(h, a);
+    if (h->validity) {
+        vah::ValidityArgs<double> v;
+        std::memset(&v, 0, sizeof(v));
+        v.nx = h->nx; v.ny = h->ny; v.nz = h->nz; v.ncx = h->ncx; v.ncy = h->ncy;
+        v.plane = (long long)h->ncx * h->ncy;
+        v.t = t + dt; v.dt = dt; v.dx = h->dx; v.dy = h->dy; v.dz = h->dz; v.etabar = h->etabar;
+        for (int n = 0; n < 16; ++n) v.qn[n] = h->vqstore.data() + h->ncell * n;
+        v.e = h->ep[c][0]; v.p = h->ep[c][1];
+        for (int m = 0; m < 4; ++m) { v.u[m] = h->up[m]; v.up[m] = h->u[m]; }
+        v.eos = h->eos;
+        for (int m = 0; m < 16; ++m) v.v[m] = h->vstore.data() + h->ncell * m;
+        if (h->physics == 0) run_validity<0>(v);
+        else if (h->physics == 1) run_validity<1>(v);
+        else run_validity<2>(v);
+    }
     for (int m = 0; m < 4; ++m) { double *tmp = h->u[m]; h->u[m] = h->up[m]; h->up[m] = tmp; }
 }
 

@@ -46,3 +46,44 @@ def test_host_build_of_device_code_matches_oracle(physics, eos, shape, pi_amp, s
         diff = np.max(np.abs(a - b))
         err = 0.0 if diff == 0 else diff / field_scale(g, fid, a)
         assert err < 1e-11, (fid, err)
+
+
+def validity_errors(g, a_get, b_get):
+    """Normwise relative differences of the 27 validity fields; the stored
+    shear combinations (ids 12-15: the trace of sigma and projections that
+    nearly cancel) are measured against the expansion rate's scale."""
+    th = np.max(np.abs(g.interior(a_get(11))))
+    errs = []
+    for vid in range(V.NUM_VALIDITY):
+        a, b = g.interior(a_get(vid)), g.interior(b_get(vid))
+        d = np.max(np.abs(a - b))
+        m = np.max(np.abs(a))
+        if 12 <= vid <= 15:
+            m = max(m, th)
+        errs.append(0.0 if d == 0 else float(d / m))
+    return errs
+
+
+@pytest.mark.parametrize("split", [0, 1], ids=["fused", "split_reference_faces"])
+@pytest.mark.parametrize("physics,eos,shape", [("pimunu", "conformal", (9, 8, 5)), ("pimunu_pi", "table", (9, 8, 5)),
+                                               ("pimunu", "table", (11, 9, 1)), ("ideal", "conformal", (9, 8, 1))])
+def test_host_build_of_validity_code_matches_oracle(physics, eos, shape, split):
+    table = V.eos_table() if eos == "table" else None
+    g = V.Grid(*shape, 0.2, 0.2, 0.2, 0.2, physics=physics, eos=eos,
+               zeta="crossover" if eos == "table" else "reference", table=table)
+    o, h = V.Oracle(g), V.HostCheck(g, split=split)
+    o.set_validity(1)
+    h.set_validity(1)
+    f = V.smooth_initial_state(g, 0.5, pi_amp=0.3)
+    V.load_state(o, f)
+    V.load_state(h, f)
+    o.set_conserved(0.5, 1)
+    h.set_conserved(0.5, 1)
+    o.set_ghost_cells()
+    for fid in V.state_ids(g.physics):
+        h.field(fid)[:] = o.field(fid)
+    for n in range(3):
+        o.step(0.5 + 0.02 * n, 0.02)
+        h.step(0.5 + 0.02 * n, 0.02)
+    errs = validity_errors(g, o.validity, h.validity)
+    assert max(errs) < 1e-10, [(k, e) for k, e in enumerate(errs) if e >= 1e-10]

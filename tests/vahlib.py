@@ -266,6 +266,14 @@ class HostCheck:
     def step(self, t, dt):
         self.L.hc_step(self.h, t, dt)
 
+    def set_validity(self, on):
+        self.L.hc_set_validity(self.h, int(on))
+
+    def validity(self, vid):
+        self.L.hc_validity_field.restype = P
+        self.L.hc_validity_field.argtypes = [C.c_void_p, I]
+        return np.ctypeslib.as_array(self.L.hc_validity_field(self.h, vid), (self.g.ncell,))
+
 
 # ------------------------------------------------------------- the library --
 import sys as _sys
