@@ -3,10 +3,14 @@
 // FileIO.cpp:14-59, {Lattice,Hydro,InitialCondition}Parameters.cpp).
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "vah.h"
@@ -163,6 +167,84 @@ extern "C" int vah_output(const double *var, double t, const char *dir, const ch
     return 0;
 }
 
+namespace {
+
+// Writes .dat snapshots on a thread of its own, so that formatting and file
+// output (the bulk of an output step's cost) overlap the following GPU steps.
+// The time loop copies each field to host memory (one synchronous copy) and
+// queues it; jobs are written in the order queued. Queued data is bounded:
+// push() waits while more than max_bytes are pending.
+class DatWriter {
+  public:
+    DatWriter(const char *dir, const LatticeParameters &lat, size_t max_bytes)
+        : dir_(dir ? dir : ""), lat_(lat), max_bytes_(max_bytes), thread_([this] { run(); }) {}
+    ~DatWriter() { finish(); }
+
+    void push(const char *name, double t, std::vector<double> &&data) {
+        std::unique_lock<std::mutex> lock(mu_);
+        space_.wait(lock, [&] { return pending_ == 0 || pending_ + data.size() * sizeof(double) <= max_bytes_; });
+        pending_ += data.size() * sizeof(double);
+        jobs_.push_back(Job{name, t, std::move(data)});
+        ready_.notify_one();
+    }
+
+    // Waits for every queued file; returns the number that could not be written.
+    int finish() {
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            if (done_) return failures_;
+            done_ = true;
+            ready_.notify_one();
+        }
+        thread_.join();
+        return failures_;
+    }
+
+  private:
+    struct Job {
+        std::string name;
+        double t;
+        std::vector<double> data;
+    };
+    void run() {
+        for (;;) {
+            Job job;
+            {
+                std::unique_lock<std::mutex> lock(mu_);
+                ready_.wait(lock, [&] { return done_ || !jobs_.empty(); });
+                if (jobs_.empty()) return;
+                job = std::move(jobs_.front());
+                jobs_.pop_front();
+            }
+            if (vah_output(job.data.data(), job.t, dir_.c_str(), job.name.c_str(), &lat_) != 0) {
+                std::fprintf(stderr, "cannot write %s/%s_%.3f.dat\n", dir_.c_str(), job.name.c_str(), job.t);
+                ++failures_;
+            }
+            std::lock_guard<std::mutex> lock(mu_);
+            pending_ -= job.data.size() * sizeof(double);
+            space_.notify_all();
+        }
+    }
+    std::string dir_;
+    LatticeParameters lat_;
+    size_t max_bytes_, pending_ = 0;
+    std::deque<Job> jobs_;
+    std::mutex mu_;
+    std::condition_variable ready_, space_;
+    bool done_ = false;
+    int failures_ = 0;
+    std::thread thread_;  // last: starts after the members it uses
+};
+
+// File names of the validity fields, as the reference's (commented-out)
+// outputs name them (HydroPlugin.cpp:48-105), in VAH_V_* order.
+const char *const kValidityNames[VAH_NUM_VALIDITY] = {
+    "knTaupiT", "knTaupiL", "knTaupi", "knTauPi", "Rpi", "RPi", "Rpi2", "RPi2", "taupi",
+    "dxux", "dyuy", "theta", "stt", "sxx", "syy", "snn", "regulations", "regMag",
+    "regTr", "regU0", "regU1", "regU2", "regU3", "regZ0", "regZ1", "regZ2", "regZ3"};
+
+}  // namespace
+
 extern "C" int vah_run_plugin(void *latticeParams, void *initCondParams, void *hydroParams, const char *rootDirectory,
                               const char *outputDir) {
     (void)rootDirectory;
@@ -254,7 +336,7 @@ extern "C" int vah_run_plugin(void *latticeParams, void *initCondParams, void *h
     const int kctr = (nz % 2 == 0) ? ncz / 2 : (ncz - 1) / 2;
     const size_t sctr = ictr + (size_t)ncx * (jctr + (size_t)ncy * kctr);
     const size_t ncell = (size_t)ncx * ncy * ncz;
-    std::vector<double> buf(ncell), ebuf(ncell), pbuf(ncell);
+    std::vector<double> ebuf(ncell), pbuf(ncell);
 
     struct Out {
         int id;
@@ -269,6 +351,16 @@ extern "C" int vah_run_plugin(void *latticeParams, void *initCondParams, void *h
         outs.insert(outs.end(), pis, pis + 10);
     }
     if (physics == VAH_PIMUNU_PI) outs.push_back({VAH_F_PI, "Pi"});
+    // VAH_VALIDITY=1: also compute the validity diagnostics every step (as the
+    // reference does) and write them with the other outputs
+    const char *venv = std::getenv("VAH_VALIDITY");
+    const bool validity = venv && std::atoi(venv) != 0;
+    if (validity && (rc = vah_event_set_validity(ev, 1)) != VAH_OK) {
+        vah_event_destroy(ev);
+        return rc;
+    }
+    DatWriter writer(outputDir, *lat, (size_t)2 * (outs.size() + (validity ? VAH_NUM_VALIDITY : 0)) * ncell *
+                                          sizeof(double));
 
     double t = t0, total_ms = 0;
     int nsteps = 0;
@@ -279,9 +371,14 @@ extern "C" int vah_run_plugin(void *latticeParams, void *initCondParams, void *h
             std::printf("n = %d:%d (t = %.3f),\t (e, p) = (%.3f, %.3f) [GeV/fm^3],\t (T = %.3f [GeV]),\t", n - 1, nt,
                         t, ebuf[sctr] * kHbarc, pbuf[sctr] * kHbarc, eos.temperature(ebuf[sctr]) * kHbarc);
             for (const Out &o : outs) {
-                if ((rc = vah_event_get_field(ev, o.id, buf.data(), 1)) != VAH_OK) break;
-                if (outputDir && vah_output(buf.data(), t, outputDir, o.name, lat) != 0)
-                    std::fprintf(stderr, "cannot write %s/%s_%.3f.dat\n", outputDir, o.name, t);
+                std::vector<double> snap(ncell);
+                if ((rc = vah_event_get_field(ev, o.id, snap.data(), 1)) != VAH_OK) break;
+                if (outputDir) writer.push(o.name, t, std::move(snap));
+            }
+            for (int v = 0; validity && rc == VAH_OK && v < VAH_NUM_VALIDITY; ++v) {
+                std::vector<double> snap(ncell);
+                if ((rc = vah_event_get_validity(ev, v, snap.data(), 1)) != VAH_OK) break;
+                if (outputDir) writer.push(kValidityNames[v], t, std::move(snap));
             }
             if (rc != VAH_OK) break;
         }
@@ -296,6 +393,7 @@ extern "C" int vah_run_plugin(void *latticeParams, void *initCondParams, void *h
     }
     if (nsteps) std::printf("Average time/step: %.3f ms\n", total_ms / nsteps);
     if (rc == VAH_ERR_NAN) std::printf("found NaN in the evolution (reference: exit(-1)).\n");
+    writer.finish();  // every queued .dat file is on disk before run() returns
     vah_event_destroy(ev);
     return rc;
 }
