@@ -329,7 +329,8 @@ def run_serve(args, rank, world, dist):
     prec = vah.VAH_FP32 if args.precision == "fp32" else vah.VAH_FP64
     flux = {"per_cell": vah.VAH_FLUX_PER_CELL, "shared": vah.VAH_FLUX_SHARED}[args.flux]
     res, lat = vah.serve(rate=50.0, duration_s=args.serve_seconds, seed=1, precision=prec, flux=flux,
-                         T0_GeV=0.4, e_floor=1e-2, t_max=100.0, ic_threads=max(2, min(host_cores(), 32)))
+                         T0_GeV=0.4, e_floor=1e-2, t_max=100.0, ic_threads=max(2, min(host_cores(), 32)),
+                         ic_on_device=1)
     line = {"metric": "events/s", "value": res["events_per_s"], "unit": "events/s", "n_gpus": 1,
             "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64-inversion" if prec == vah.VAH_FP32 else "f64",
@@ -337,7 +338,8 @@ def run_serve(args, rank, world, dist):
             "config": {"workload": "vah serving: Poisson 50 events/s, 70% 2+1D side U[61,261], 30% 3+1D "
                                    "81^2x41..161^2x81, b~U[0,14], dx=0.2, deta=0.2, dtau=0.02, MC-Glauber peak "
                                    "T0=0.4 GeV + 0.01 fm^-4 floor, table EoS, eta/s=0.16, retired at max T<150 MeV "
-                                   "over converged cells (timeout tau=100 fm/c)",
+                                   "over converged cells (timeout tau=100 fm/c); ICs generated on the GPU at "
+                                   "admission",
                        "arrival_window_s": args.serve_seconds, "faces": args.flux},
             "latency_p50_s": res["p50_s"], "latency_p99_s": res["p99_s"], "serve": res}
     print(json.dumps(line), flush=True)

@@ -172,6 +172,42 @@ __global__ void hot_init_kernel(const S *e, unsigned char *hot, double e_freeze,
     }
 }
 
+// MC-Glauber deposit on the device: v(x, y) = sum over participants of
+// exp(-r^2 / (2 w^2)) (cut at r = 8 w, as the host generator), one thread per
+// transverse cell; the maximum goes to maxbits (positive doubles order like
+// their bit patterns).
+__global__ void glauber_deposit_kernel(const double *__restrict__ pxy, int np, double inv2w2, double cut2, int nx,
+                                       int ny, double dx, double dy, double *vxy, unsigned long long *maxbits) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nx * ny; c += gridDim.x * blockDim.x) {
+        const int i = c % nx, j = c / nx;
+        const double x = (i - (nx - 1) / 2.) * dx, y = (j - (ny - 1) / 2.) * dy;
+        double v = 0;
+        for (int p = 0; p < np; ++p) {
+            const double rx = x - pxy[2 * p], ry = y - pxy[2 * p + 1];
+            const double r2 = rx * rx + ry * ry;
+            if (r2 < cut2) v += exp(-r2 * inv2w2);
+        }
+        vxy[c] = v;
+        atomicMax(maxbits, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// e(x, y, eta) = e_peak v / max v * f(eta) + e_floor into the slot's interior
+// (a flat floor when no nucleon collided).
+template <typename S>
+__global__ void glauber_fill_kernel(const double *__restrict__ vxy, const unsigned long long *__restrict__ maxbits,
+                                    const double *__restrict__ feta, int nx, int ny, int nz, double e_peak,
+                                    double e_floor, S *e) {
+    const double vmax = __longlong_as_double((long long)*maxbits);
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const long long t = c % ((long long)nx * ny);
+        const int k = (int)(c / ((long long)nx * ny)), i = (int)(t % nx), j = (int)(t / nx);
+        const double exy = vmax > 0 ? e_peak * vxy[t] / vmax : 0.0;
+        e[(i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * (k + 2))] = (S)(exy * feta[k] + e_floor);
+    }
+}
+
 // Per-slot maximum of e over the interior cells whose latest inversion
 // converged (positive doubles order like their bit patterns), for the
 // freeze-out test. A cell whose inversion fell back holds e = 0.999 e_prev and
@@ -573,19 +609,59 @@ vah::FieldSet<S> fs(S *const *p, int n) {
     return f;
 }
 
-// Initial state of a slot: e interior uploaded, p = EoS(e), u = 1, pi = 0,
-// conserved variables, ghost layers (the vah_event_init_from_e sequence).
+// Device-generated initial energy density (vah_batch_add_glauber) into the
+// slot's e interior; scratch from the batch's pool, freed in stream order.
 template <typename S>
-int init_slot(vah_batch *b, int slot, double t0, const double *e_interior, int pl_mode) {
+int glauber_slot(vah_batch *b, const SlotDesc<S> &d, const vah_lattice &lat, const vah_glauber &g) {
+    std::vector<double> pxy(2 * (size_t)(2 * g.A));
+    int np = 0;
+    int rc = vah_ic_mc_glauber_participants(g.b, g.sigma_nn_fm2, g.A, g.ws_R, g.ws_a, g.seed, pxy.data(), 2 * g.A, &np);
+    if (rc != VAH_OK) return rc;
+    std::vector<double> feta(lat.nz, 1.0);
+    if (lat.nz > 1 && (rc = vah_ic_longitudinal(lat.nz, lat.dz, g.eta_flat, g.sigma_eta, feta.data())) != VAH_OK)
+        return rc;
+    const size_t nxy = (size_t)lat.nx * lat.ny;
+    const size_t bytes = 256 + sizeof(double) * (2 * (size_t)std::max(np, 1) + nxy + lat.nz);
+    char *scratch = nullptr;
+    VAH_TRY(cudaMallocFromPoolAsync((void **)&scratch, bytes, b->pool, b->stream));
+    unsigned long long *maxbits = (unsigned long long *)scratch;
+    double *d_pxy = (double *)(scratch + 256), *d_v = d_pxy + 2 * (size_t)std::max(np, 1), *d_f = d_v + nxy;
+    VAH_TRY(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), b->stream));
+    if (np) VAH_TRY(cudaMemcpyAsync(d_pxy, pxy.data(), sizeof(double) * 2 * np, cudaMemcpyHostToDevice, b->stream));
+    VAH_TRY(cudaMemcpyAsync(d_f, feta.data(), sizeof(double) * lat.nz, cudaMemcpyHostToDevice, b->stream));
+    const int block = 128;
+    vah::glauber_deposit_kernel<<<(int)std::min<size_t>((nxy + block - 1) / block, 148 * 16), block, 0, b->stream>>>(
+        d_pxy, np, 1.0 / (2 * g.width * g.width), 64 * g.width * g.width, lat.nx, lat.ny, lat.dx, lat.dy, d_v,
+        maxbits);
+    VAH_TRY(cudaGetLastError());
+    vah::glauber_fill_kernel<S><<<(int)std::min<size_t>((nxy * lat.nz + block - 1) / block, 148 * 16), block, 0,
+                                  b->stream>>>(d_v, maxbits, d_f, lat.nx, lat.ny, lat.nz, g.e_peak, g.e_floor,
+                                               d.ep[0][0]);
+    VAH_TRY(cudaGetLastError());
+    VAH_TRY(cudaFreeAsync(scratch, b->stream));
+    return VAH_OK;
+}
+
+// Initial state of a slot: e interior uploaded (or generated on the device),
+// p = EoS(e), u = 1, pi = 0, conserved variables, ghost layers (the
+// vah_event_init_from_e sequence).
+template <typename S>
+int init_slot(vah_batch *b, int slot, double t0, const double *e_interior, const vah_glauber *glauber, int pl_mode) {
     vah_batch::Slot &sl = b->slots[slot];
     SlotDesc<S> &d = *desc_host<S>(b, slot);
     const int nx = sl.lat.nx, ny = sl.lat.ny, nz = sl.lat.nz;
-    std::vector<S> stage((size_t)nx * ny * nz);
-    for (size_t k = 0; k < stage.size(); ++k) stage[k] = (S)e_interior[k];
-    for (int k = 0; k < nz; ++k) {
-        S *dst = d.ep[0][0] + 2 + (size_t)d.ncx * (2 + (size_t)d.ncy * (k + 2));
-        VAH_TRY(cudaMemcpy2DAsync(dst, d.ncx * sizeof(S), stage.data() + (size_t)nx * ny * k, nx * sizeof(S),
-                                  nx * sizeof(S), ny, cudaMemcpyHostToDevice, b->stream));
+    std::vector<S> stage;
+    if (glauber) {
+        const int rc = glauber_slot<S>(b, d, sl.lat, *glauber);
+        if (rc != VAH_OK) return rc;
+    } else {
+        stage.resize((size_t)nx * ny * nz);
+        for (size_t k = 0; k < stage.size(); ++k) stage[k] = (S)e_interior[k];
+        for (int k = 0; k < nz; ++k) {
+            S *dst = d.ep[0][0] + 2 + (size_t)d.ncx * (2 + (size_t)d.ncy * (k + 2));
+            VAH_TRY(cudaMemcpy2DAsync(dst, d.ncx * sizeof(S), stage.data() + (size_t)nx * ny * k, nx * sizeof(S),
+                                      nx * sizeof(S), ny, cudaMemcpyHostToDevice, b->stream));
+        }
     }
     S *qs[16];
     for (int n = 0; n < 16; ++n) qs[n] = n < b->nq || (n == 15 && b->nq == 16) ? d.q[n] : nullptr;
@@ -745,9 +821,14 @@ extern "C" int vah_batch_event_bytes(const vah_batch *b, const vah_lattice *lat,
     return VAH_OK;
 }
 
-extern "C" int vah_batch_add(vah_batch *b, const vah_lattice *lat, const vah_hydro *hydro, double dt,
-                             const double *e_interior, int pl_mode, int *slot_out) {
-    if (!b || !lat || !hydro || !e_interior || !slot_out || !(dt > 0) || !(hydro->t0 > 0)) return VAH_ERR_ARG;
+namespace {
+
+// Admission shared by vah_batch_add and vah_batch_add_glauber: footprint
+// check, slot memory, descriptors, initial state.
+int add_slot(vah_batch *b, const vah_lattice *lat, const vah_hydro *hydro, double dt, const double *e_interior,
+             const vah_glauber *glauber, int pl_mode, int *slot_out) {
+    if (!b || !lat || !hydro || (!e_interior && !glauber) || !slot_out || !(dt > 0) || !(hydro->t0 > 0))
+        return VAH_ERR_ARG;
     if (lat->nx < 1 || lat->ny < 1 || lat->nz < 1 || !(hydro->eta_over_s > 0)) return VAH_ERR_ARG;
     const size_t bytes = event_bytes(b, lat);
     if (b->used + bytes > b->capacity) return VAH_ERR_FULL;
@@ -770,8 +851,8 @@ extern "C" int vah_batch_add(vah_batch *b, const vah_lattice *lat, const vah_hyd
     b->used += bytes;
     int rc = b->elem == sizeof(float) ? fill_slot<float>(b, slot) : fill_slot<double>(b, slot);
     if (rc == VAH_OK)
-        rc = b->elem == sizeof(float) ? init_slot<float>(b, slot, hydro->t0, e_interior, pl_mode)
-                                      : init_slot<double>(b, slot, hydro->t0, e_interior, pl_mode);
+        rc = b->elem == sizeof(float) ? init_slot<float>(b, slot, hydro->t0, e_interior, glauber, pl_mode)
+                                      : init_slot<double>(b, slot, hydro->t0, e_interior, glauber, pl_mode);
     if (rc != VAH_OK) {
         vah_batch_remove(b, slot);
         return rc;
@@ -779,6 +860,21 @@ extern "C" int vah_batch_add(vah_batch *b, const vah_lattice *lat, const vah_hyd
     b->dirty = true;
     *slot_out = slot;
     return VAH_OK;
+}
+
+}  // namespace
+
+extern "C" int vah_batch_add(vah_batch *b, const vah_lattice *lat, const vah_hydro *hydro, double dt,
+                             const double *e_interior, int pl_mode, int *slot_out) {
+    if (!e_interior) return VAH_ERR_ARG;
+    return add_slot(b, lat, hydro, dt, e_interior, nullptr, pl_mode, slot_out);
+}
+
+extern "C" int vah_batch_add_glauber(vah_batch *b, const vah_lattice *lat, const vah_hydro *hydro, double dt,
+                                     const vah_glauber *g, int pl_mode, int *slot_out) {
+    if (!g || g->A < 1 || !(g->width > 0) || !(g->e_peak > 0) || !(g->e_floor >= 0)) return VAH_ERR_ARG;
+    if (lat && lat->nz > 1 && !(g->sigma_eta > 0)) return VAH_ERR_ARG;
+    return add_slot(b, lat, hydro, dt, nullptr, g, pl_mode, slot_out);
 }
 
 extern "C" int vah_batch_remove(vah_batch *b, int slot) {

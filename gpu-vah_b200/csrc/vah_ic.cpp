@@ -114,10 +114,14 @@ extern "C" int vah_ic_optical_glauber(int nx, int ny, double dx, double dy, doub
     return VAH_OK;
 }
 
-extern "C" int vah_ic_mc_glauber(int nx, int ny, double dx, double dy, double b, double sigma_nn_fm2, int A,
-                                 double ws_R, double ws_a, double width, unsigned long long seed, double e_peak,
-                                 double e_floor, double *e_xy, int *npart_out) {
-    if (nx < 1 || ny < 1 || !e_xy || !(width > 0) || A < 1) return VAH_ERR_ARG;
+namespace {
+
+// Participant positions of one seeded MC-Glauber collision: nucleons drawn from
+// the two Woods-Saxon nuclei displaced by +-b/2 along x; a nucleon
+// participates if some nucleon of the other nucleus lies within
+// sqrt(sigma_NN / pi) in the transverse plane.
+void participants(double b, double sigma_nn_fm2, int A, double ws_R, double ws_a, unsigned long long seed,
+                  std::vector<double> &px, std::vector<double> &py) {
     std::vector<double> xa, ya, xb, yb;
     Rng ra(seed * 2 + 0x1234567ull), rb(seed * 2 + 1 + 0x1234567ull);
     sample_nucleus(ra, A, ws_R, ws_a, +b / 2, xa, ya);
@@ -129,9 +133,34 @@ extern "C" int vah_ic_mc_glauber(int nx, int ny, double dx, double dy, double b,
             const double ddx = xa[m] - xb[n], ddy = ya[m] - yb[n];
             if (ddx * ddx + ddy * ddy < d2max) pa[m] = pb[n] = 1;
         }
-    std::vector<double> px, py;
+    px.clear();
+    py.clear();
     for (int m = 0; m < A; ++m) if (pa[m]) { px.push_back(xa[m]); py.push_back(ya[m]); }
     for (int n = 0; n < A; ++n) if (pb[n]) { px.push_back(xb[n]); py.push_back(yb[n]); }
+}
+
+}  // namespace
+
+extern "C" int vah_ic_mc_glauber_participants(double b, double sigma_nn_fm2, int A, double ws_R, double ws_a,
+                                              unsigned long long seed, double *xy, int max, int *n_out) {
+    if (!xy || !n_out || A < 1 || max < 0) return VAH_ERR_ARG;
+    std::vector<double> px, py;
+    participants(b, sigma_nn_fm2, A, ws_R, ws_a, seed, px, py);
+    *n_out = (int)px.size();
+    if ((int)px.size() > max) return VAH_ERR_TOO_LARGE;
+    for (size_t p = 0; p < px.size(); ++p) {
+        xy[2 * p] = px[p];
+        xy[2 * p + 1] = py[p];
+    }
+    return VAH_OK;
+}
+
+extern "C" int vah_ic_mc_glauber(int nx, int ny, double dx, double dy, double b, double sigma_nn_fm2, int A,
+                                 double ws_R, double ws_a, double width, unsigned long long seed, double e_peak,
+                                 double e_floor, double *e_xy, int *npart_out) {
+    if (nx < 1 || ny < 1 || !e_xy || !(width > 0) || A < 1) return VAH_ERR_ARG;
+    std::vector<double> px, py;
+    participants(b, sigma_nn_fm2, A, ws_R, ws_a, seed, px, py);
     if (npart_out) *npart_out = (int)px.size();
     const double inv2w2 = 1.0 / (2 * width * width), cut2 = 64 * width * width;
     double emax = 0;

@@ -109,6 +109,7 @@ extern "C" int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res,
     std::atomic<int> next_build{0};
     std::atomic<bool> stop{false};
     auto worker = [&]() {
+        if (cfg->ic_on_device) return;  // the IC is generated at admission
         for (;;) {
             const int k = next_build.fetch_add(1);
             if (k >= (int)reqs.size() || stop) return;
@@ -148,13 +149,21 @@ extern "C" int vah_serve_run(const vah_serve_config *cfg, vah_serve_result *res,
         bool refused = false;
         while (next_admit < (int)reqs.size() && !refused) {
             Request &r = reqs[next_admit];
-            {
+            if (cfg->ic_on_device) {
+                if (seconds_since(t_start) < r.arrival) break;
+            } else {
                 std::unique_lock<std::mutex> lock(mu);
                 if (!r.ready) break;
             }
             vah_hydro hy{cfg->t0, cfg->eta_over_s, cfg->Tf_GeV};
             int slot = -1;
-            int a = vah_batch_add(batch, &r.lat, &hy, cfg->dt, r.e.data(), VAH_PL_ISOTROPIC, &slot);
+            int a;
+            if (cfg->ic_on_device) {
+                const vah_glauber g{r.b, 4.2, 197, 6.38, 0.535, 0.5, r.seed, e_peak, cfg->e_floor, 1.5, 1.3};
+                a = vah_batch_add_glauber(batch, &r.lat, &hy, cfg->dt, &g, VAH_PL_ISOTROPIC, &slot);
+            } else {
+                a = vah_batch_add(batch, &r.lat, &hy, cfg->dt, r.e.data(), VAH_PL_ISOTROPIC, &slot);
+            }
             if (a == VAH_ERR_FULL) {
                 refused = live.empty() ? false : true;
                 if (live.empty()) {  // larger than the whole batch: reject the request

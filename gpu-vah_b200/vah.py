@@ -80,7 +80,7 @@ EXPORTS = ["vah_version", "vah_eos_table_build", "vah_event_create", "vah_event_
            "vah_event_kernel_time", "vah_rk2_step_host", "vah_ic_optical_glauber", "vah_ic_mc_glauber",
            "vah_ic_longitudinal", "vah_event_autotune", "vah_batch_autotune",
            "vah_batch_freezeout_volume", "vah_batch_fallback_mask", "vah_event_set_validity",
-           "vah_event_get_validity"]
+           "vah_event_get_validity", "vah_batch_add_glauber", "vah_ic_mc_glauber_participants"]
 
 _lib = None
 
@@ -269,6 +269,8 @@ def _batch_lib():
     if not getattr(L, "_batch_ready", False):
         L.vah_batch_create.argtypes = [C.POINTER(Options), P, C.c_size_t, C.POINTER(C.c_void_p)]
         L.vah_batch_autotune.argtypes = [C.c_void_p, I, C.POINTER(TuneReport)]
+        L.vah_batch_add_glauber.argtypes = [C.c_void_p, C.POINTER(Lattice), C.POINTER(Hydro), D, C.POINTER(Glauber), I,
+                                            C.POINTER(I)]
         for name in ("vah_batch_destroy", "vah_batch_sync"):
             getattr(L, name).argtypes = [C.c_void_p]
         L.vah_batch_event_bytes.argtypes = [C.c_void_p, C.POINTER(Lattice), C.POINTER(C.c_size_t)]
@@ -283,6 +285,11 @@ def _batch_lib():
         L.vah_batch_kernel_time.argtypes = [C.c_void_p, P, C.POINTER(C.c_longlong)]
         L._batch_ready = True
     return L
+
+
+class Glauber(C.Structure):
+    _fields_ = [("b", D), ("sigma_nn_fm2", D), ("A", I), ("ws_R", D), ("ws_a", D), ("width", D),
+                ("seed", C.c_ulonglong), ("e_peak", D), ("e_floor", D), ("eta_flat", D), ("sigma_eta", D)]
 
 
 class Batch:
@@ -324,6 +331,20 @@ class Batch:
         if rc == VAH_ERR_FULL:
             return None
         check(rc, "vah_batch_add")
+        self.shapes[slot.value] = (nx, ny, nz)
+        return slot.value
+
+    def add_glauber(self, nx, ny, nz, dx, dy, dz, t0, dt, eta_over_s, b, seed, e_peak, e_floor=1e-3, sigma_nn_fm2=4.2,
+                    A=197, R=6.38, a=0.535, width=0.5, eta_flat=1.5, sigma_eta=1.3, pl_mode=VAH_PL_ISOTROPIC):
+        """An event whose MC-Glauber initial condition is generated on the device; None when full."""
+        g = Glauber(b, sigma_nn_fm2, A, R, a, width, seed, e_peak, e_floor, eta_flat, sigma_eta)
+        slot = C.c_int()
+        rc = self.L.vah_batch_add_glauber(self.b, C.byref(Lattice(nx, ny, nz, dx, dy, dz)),
+                                          C.byref(Hydro(t0, eta_over_s, 0.15)), dt, C.byref(g), pl_mode,
+                                          C.byref(slot))
+        if rc == VAH_ERR_FULL:
+            return None
+        check(rc, "vah_batch_add_glauber")
         self.shapes[slot.value] = (nx, ny, nz)
         return slot.value
 
@@ -393,7 +414,8 @@ class ServeConfig(C.Structure):
                 ("side2_max", I), ("side3_min", I), ("side3_max", I), ("nz3_min", I), ("nz3_max", I), ("dx", D),
                 ("deta", D), ("b_max", D), ("t0", D), ("dt", D), ("eta_over_s", D), ("T0_GeV", D), ("Tf_GeV", D),
                 ("t_max", D), ("physics", I), ("eos", I), ("precision", I), ("flux", I), ("device", I),
-                ("capacity_bytes", C.c_size_t), ("chunk_steps", I), ("ic_threads", I), ("e_floor", D)]
+                ("capacity_bytes", C.c_size_t), ("chunk_steps", I), ("ic_threads", I), ("e_floor", D),
+                ("ic_on_device", I)]
 
 
 class ServeResult(C.Structure):
@@ -415,7 +437,7 @@ def serve(**kw):
                side3_max=161, nz3_min=41, nz3_max=81, dx=0.2, deta=0.2, b_max=14.0, t0=0.25, dt=0.02,
                eta_over_s=0.16, T0_GeV=0.4, Tf_GeV=0.150, t_max=100.0, physics=VAH_PIMUNU_PI, eos=VAH_EOS_TABLE,
                precision=VAH_FP64, flux=VAH_FLUX_PER_CELL, device=0, capacity_bytes=120 << 30, chunk_steps=10,
-               ic_threads=16, e_floor=1e-2)
+               ic_threads=16, e_floor=1e-2, ic_on_device=1)
     cfg.update(kw)
     c = ServeConfig(**cfg)
     r = ServeResult()

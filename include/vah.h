@@ -290,6 +290,22 @@ int vah_batch_event_bytes(const vah_batch *b, const vah_lattice *lat, size_t *by
 int vah_batch_add(vah_batch *b, const vah_lattice *lat, const vah_hydro *hydro, double dt, const double *e_interior,
                   int pl_mode, int *slot);
 int vah_batch_remove(vah_batch *b, int slot);
+/* An event whose initial energy density is generated on the device (no
+ * reference counterpart; the reference builds ICs on the host,
+ * InitialConditions.cpp:196-292): the MC-Glauber collision of
+ * vah_ic_mc_glauber (participants sampled on the host, their Gaussians
+ * deposited on the GPU), e(x, y, eta) = e_peak v(x,y) / max v * f(eta) +
+ * e_floor with f from vah_ic_longitudinal (1 in 2+1D); then as vah_batch_add. */
+typedef struct vah_glauber {
+    double b, sigma_nn_fm2;
+    int A;
+    double ws_R, ws_a, width;
+    unsigned long long seed;
+    double e_peak, e_floor;
+    double eta_flat, sigma_eta;
+} vah_glauber;
+int vah_batch_add_glauber(vah_batch *b, const vah_lattice *lat, const vah_hydro *hydro, double dt,
+                          const vah_glauber *g, int pl_mode, int *slot);
 /* nsteps RK2 steps of every admitted event (asynchronous). */
 int vah_batch_step(vah_batch *b, int nsteps);
 int vah_batch_sync(vah_batch *b);
@@ -351,6 +367,7 @@ typedef struct vah_serve_config {
     size_t capacity_bytes;
     int chunk_steps, ic_threads;
     double e_floor;  /* energy density added to every initial cell, fm^-4 (the reference adds 1e-3) */
+    int ic_on_device; /* 1: admission generates each IC on the GPU (vah_batch_add_glauber); 0: host threads build it */
 } vah_serve_config;
 
 typedef struct vah_serve_result {
@@ -376,6 +393,10 @@ int vah_ic_optical_glauber(int nx, int ny, double dx, double dy, double b, doubl
 int vah_ic_mc_glauber(int nx, int ny, double dx, double dy, double b, double sigma_nn_fm2, int A, double ws_R,
                       double ws_a, double width, unsigned long long seed, double e_peak, double e_floor,
                       double *e_xy, int *npart_out);
+/* The participant positions of vah_ic_mc_glauber's collision (x, y pairs in
+ * xy, at most `max`; *n_out is their number, VAH_ERR_TOO_LARGE if above max). */
+int vah_ic_mc_glauber_participants(double b, double sigma_nn_fm2, int A, double ws_R, double ws_a,
+                                   unsigned long long seed, double *xy, int max, int *n_out);
 /* f(eta) = 1 for |eta| < eta_flat, exp(-(|eta|-eta_flat)^2 / (2 sigma_eta^2)) beyond. */
 int vah_ic_longitudinal(int nz, double dz, double eta_flat, double sigma_eta, double *f_eta);
 

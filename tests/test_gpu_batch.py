@@ -160,3 +160,28 @@ def test_freezeout_volume_does_not_depend_on_the_mix():
     assert np.all(v_mix[slots] >= 0.0)
     mixed.close()
     alone.close()
+
+
+@pytest.mark.parametrize("nz,dz", [(1, 0.2), (9, 0.3)], ids=["2+1D", "3+1D"])
+def test_device_glauber_ic_matches_the_host_generator(nz, dz):
+    """vah_batch_add_glauber deposits the participants' Gaussians on the GPU;
+    the energy density equals the host generator's (times the longitudinal
+    profile, plus the floor) up to the last bits of exp."""
+    tab = V.eos_table()
+    nx, ny, dx = 43, 37, 0.3
+    e_peak = vah.table_energy_density(tab, 0.5 / vah.HBARC)
+    batch = vah.Batch(table=tab, capacity_bytes=2 << 30)
+    slot = batch.add_glauber(nx, ny, nz, dx, dx, dz, 0.4, 0.01, 0.16, b=6.0, seed=21, e_peak=e_peak, e_floor=1e-2)
+    exy, npart = vah.mc_glauber(nx, ny, dx, dx, 6.0, 21, e_peak=e_peak, e_floor=0.0)
+    f = vah.longitudinal(nz, dz) if nz > 1 else np.ones(1)
+    host = (f[:, None] * exy[None, :]).ravel() + 1e-2
+    dev = batch.get_field(slot, 16, False)
+    assert npart > 10
+    assert np.max(np.abs(dev - host)) <= 1e-13 * np.max(host)
+    # and it evolves like the host-built event
+    ref = batch.add(nx, ny, nz, dx, dx, dz, 0.4, 0.01, 0.16, host)
+    batch.step(5)
+    for fid in (16, 18, 19, 4):
+        a, b_ = batch.get_field(slot, fid, False), batch.get_field(ref, fid, False)
+        assert rel(a, b_, 1e-3 * np.max(host)) < 1e-11, fid
+    batch.close()
