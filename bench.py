@@ -139,6 +139,30 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# --------------------------------------------------------------- ranks ----
+# N > 1: one process per GPU, each running its own replica (the events are
+# independent: no data-path collective). Only the timing crosses ranks.
+def max_over_ranks(dist, seconds, device="cuda"):
+    """The slowest rank's time (the whole job ends when it does)."""
+    if dist is None:
+        return seconds
+    import torch
+
+    t = torch.tensor([seconds], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, seconds):
+    """Units all ranks processed per second of the slowest rank (weak scaling)."""
+    return world * units_per_rank / seconds
+
+
+def rank_seed(rank, base):
+    """Each replica runs its own seeded event(s)."""
+    return base + rank
+
+
 # ------------------------------------------------------------ CPU baseline --
 def _ref_worker(args):
     """Run the reference's own CPU step (oracle/_ref) on the sample slab."""
@@ -270,7 +294,7 @@ def run_batch(args, rank, world, dist):
                       capacity_bytes=150 << 30)
     e_peak = vah.table_energy_density(table, 0.6 / vah.HBARC)
     cells = 0
-    for side, b, seed in batch_events(args.events, 1000 + rank):
+    for side, b, seed in batch_events(args.events, rank_seed(rank, 1000)):
         exy, _ = vah.mc_glauber(side, side, DX, DX, b, seed, e_peak=e_peak)
         slot = batch.add(side, side, 1, DX, DX, DZ, T0, BATCH_DT, ETA_S, exy)
         assert slot is not None, "batch capacity"
@@ -289,17 +313,13 @@ def run_batch(args, rank, world, dist):
         batch.step(args.steps)
         end.record(stream)
         torch.cuda.synchronize()
-    elapsed = start.elapsed_time(end) / 1000.0
-    if dist is not None:
-        tt = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt.item())
+    elapsed = max_over_ranks(dist, start.elapsed_time(end) / 1000.0)
     batch.close()
     if rank != 0:
         return
     w = 4 if prec == vah.VAH_FP32 else 8
     bpc = (5 * NQ + 32) * w
-    value = world * cells * args.steps / elapsed
+    value = whole_job_rate(world, cells * args.steps, elapsed)
     peak, peak_kind = measured_peaks()
     achieved = bpc * cells * args.steps / elapsed / 1e9
     line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -454,7 +474,7 @@ def run_vah(args, rank, world, dist):
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()  # a real stream handle: the library queues its kernels on it
     table = vah.eos_table()
-    e0 = initial_energy_density(vah, table, seed=1 + rank)
+    e0 = initial_energy_density(vah, table, seed=rank_seed(rank, 1))
     prec = vah.VAH_FP32 if args.precision == "fp32" else vah.VAH_FP64
     ev = vah.Event(NX, NY, NZ, DX, DX, DZ, ETA_S, physics=vah.VAH_PIMUNU_PI, eos=vah.VAH_EOS_TABLE,
                    zeta=vah.VAH_ZETA_CROSSOVER, table=table, t0=T0, device=local, stream=stream.cuda_stream,
@@ -489,12 +509,9 @@ def run_vah(args, rank, world, dist):
     kms, launches = ev.kernel_time()
     ev.set_timing(False)
     ev.sync()
-    if dist is not None:
-        tt = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt.item())
+    elapsed = max_over_ranks(dist, elapsed)
     cells = NX * NY * NZ
-    value = world * cells * args.steps / elapsed
+    value = whole_job_rate(world, cells * args.steps, elapsed)
 
     # end to end through the host-buffer entry point (pinned host state, H2D + step + D2H per step)
     ids = list(range(16)) + list(range(16, 26))
@@ -507,12 +524,8 @@ def run_vah(args, rank, world, dist):
     for n in range(args.e2e_steps):
         ev.step_host(t, DT, ptrs)
         t += DT
-    e2e_s = time.perf_counter() - a
-    if dist is not None:
-        tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e_value = world * cells * args.e2e_steps / e2e_s
+    e2e_s = max_over_ranks(dist, time.perf_counter() - a)
+    e2e_value = whole_job_rate(world, cells * args.e2e_steps, e2e_s)
     state_bytes = sum(h.numel() * 8 for h in host.values())
     stats = ev.stats()
     ev.close()
