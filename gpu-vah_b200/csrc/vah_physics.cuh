@@ -271,6 +271,52 @@ VAH_HD int newton_uT(const InvSetup &s, double uT0, double &uT) {
     return 1;
 }
 
+// One Newton iteration from w, straight-line (the exits are tested after the
+// arithmetic, so that two independent iterations can be interleaved by the
+// scheduler): 0 = converged to next, 1 = the reference falls back, 2 = go on
+// from next. The same operations as newton_uT's loop body.
+VAH_HD int newton_step(const InvSetup &s, double w, double &next) {
+    const double w2 = 1 + w * w;
+    const double r = rsqrt_d(w2);
+    const double v = w * r;
+    const double e = s.c0 - v * s.x * s.mbt;
+    const double g = s.bL + s.b * (0.5 * (e - s.pl) + 1.5 * s.bulk);
+    const double r3 = r * r * r;
+    const double f = v * g - s.bT;
+    double fp = r3 * g + v * s.b * (0.5 * (-s.bT * r3));
+    if (fabs(fp) == 0.0) fp = 1.e-16;
+    next = w - f / fp;
+    if (e < 0.0) return 1;
+    if (isnan(next) || isinf(next) || next < 0 || next > 9.0072e+15) return 1;
+    return fabs(next - w) <= 1.e-7 * fabs(next) ? 0 : 2;
+}
+
+// Two independent Newton solves in lockstep (same iterates as two newton_uT
+// calls, one loop): st = 0 converged (root in u), 1 fallback.
+VAH_HD void newton_uT2(const InvSetup &A, const InvSetup &B, double g0, double g1, double &u0, double &u1, int &st0,
+                       int &st1) {
+    double w0 = g0, w1 = g1;
+    st0 = st1 = 2;
+    for (int it = 0; it < 10000; ++it) {
+        double n0 = w0, n1 = w1;
+        const int c0 = newton_step(A, w0, n0);
+        const int c1 = newton_step(B, w1, n1);
+        if (st0 == 2) {
+            st0 = c0;
+            w0 = n0;
+        }
+        if (st1 == 2) {
+            st1 = c1;
+            w1 = n1;
+        }
+        if (st0 != 2 && st1 != 2) break;
+    }
+    if (st0 == 2) st0 = 1;  // 10^4 iterations without convergence
+    if (st1 == 2) st1 = 1;
+    u0 = w0;
+    u1 = w1;
+}
+
 // The full inversion. Returns 0 (converged), 1 (fallback) or 2 (a NaN
 // reached e or u). out = {e, p, ut, ux, uy, un}.
 template <int PHYS>
@@ -336,13 +382,29 @@ VAH_HD int face_velocity(const InvSetup &s, double ePrev, double uT0, int dir, d
 // sR/sL: the inversion set-ups of qR/qL; ePrev, uT: the evaluating cell's
 // fallback energy and Newton guess.
 // Returns the number of the two inversions that fell back; bit 8 flags a NaN.
+// The velocity of a converged solve, as face_velocity (status 0 or 2).
+VAH_HD int face_velocity_of(const InvSetup &s, double uT, int dir, double *v) {
+    double vv;
+    if (dir == 2) {
+        vv = s.F;
+    } else {
+        const double C = sqrt(1.0 + uT * uT);
+        vv = uT * (dir == 0 ? s.m1 : s.m2) * s.x / (s.mbt * C);
+    }
+    *v = vv;
+    return (isnan(vv) || isnan(s.c0)) ? 2 : 0;
+}
+
 template <int PHYS>
 VAH_HD int face_flux_setup(const InvSetup &sR, const InvSetup &sL, const double *qR, const double *qL, int dir,
                            double ePrev, double uT, double *H) {
     constexpr int NQ = Phys<PHYS>::NQ;
-    double vR, vL;
-    const int stR = face_velocity(sR, ePrev, uT, dir, &vR);
-    const int stL = face_velocity(sL, ePrev, uT, dir, &vL);
+    // both states' Newton solves from this guess, in lockstep
+    double uR, uL, vR = 0.0, vL = 0.0;
+    int nR, nL;
+    newton_uT2(sR, sL, uT, uT, uR, uL, nR, nL);
+    const int stR = nR != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sR, uR, dir, &vR);
+    const int stL = nL != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sL, uL, dir, &vL);
     const double a = fmax(fabs(vL), fabs(vR));
 #pragma unroll
     for (int n = 0; n < NQ; ++n) H[n] = 0.5 * (vR * qR[n] + vL * qL[n] - a * (qR[n] - qL[n]));
