@@ -52,6 +52,8 @@ struct vah_event {
     int tev_used;
     double kernel_ms;
     long long kernel_launches;
+    cudaStream_t s_in, s_out;         // copy streams of the pipelined host-buffer step (created on first use)
+    std::vector<cudaEvent_t> pev;     // its slab events
 };
 
 namespace {
@@ -107,6 +109,9 @@ void free_all(vah_event *ev) {
     for (int m = 0; m < VAH_NUM_VALIDITY; ++m) cudaFree(ev->vd[m]);
     for (int n = 0; n < 16; ++n) cudaFree(ev->vq[n]);
     for (cudaEvent_t e : ev->tev) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev->pev) cudaEventDestroy(e);
+    if (ev->s_in) cudaStreamDestroy(ev->s_in);
+    if (ev->s_out) cudaStreamDestroy(ev->s_out);
     if (ev->own_stream && ev->stream) cudaStreamDestroy(ev->stream);
 }
 
@@ -126,6 +131,8 @@ void fill_common(const vah_event *ev, StageArgs<S> &a) {
     a.nx = ev->lat.nx;
     a.ny = ev->lat.ny;
     a.nz = ev->lat.nz;
+    a.k0 = 0;
+    a.k1 = ev->lat.nz;
     a.ncx = ev->ncx;
     a.ncy = ev->ncy;
     a.plane = (long long)ev->ncx * ev->ncy;
@@ -209,6 +216,8 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->steps = 0;
     ev->last_t = hydro->t0;
     ev->d_stage64 = nullptr;
+    ev->s_in = nullptr;
+    ev->s_out = nullptr;
     ev->validity = false;
     memset(ev->vd, 0, sizeof(ev->vd));
     memset(ev->vq, 0, sizeof(ev->vq));
@@ -435,18 +444,11 @@ void stage1_args(const vah_event *ev, double t, double dt, StageArgs<S> &a) {
     a.pout = (S *)ev->ep[o][1];
 }
 
+// Stage 2: qS, uS, (e, p)[o], u -> q (in place, with the convex
+// combination), up buffer (becomes u^{n+1}), (e, p)[c].
 template <typename S>
-int rk2_step_t(vah_event *ev, double t, double dt) {
+void stage2_args(const vah_event *ev, double t, double dt, StageArgs<S> &a) {
     const int c = ev->cur, o = 1 - ev->cur;
-    if (ev->validity)  // the diagnostics read P_L, pi, Pi as they are at the start of the step
-        for (int n = VAH_F_PL; n < ev->nq; ++n)
-            VAH_TRY(cudaMemcpyAsync(ev->vq[n], ev->q[n], ev->ncell * sizeof(S), cudaMemcpyDeviceToDevice, ev->stream));
-    StageArgs<S> a;
-    stage1_args(ev, t, dt, a);
-    int rc = timed_launch(ev, a);
-    if (rc != VAH_OK) return rc;
-    // stage 2: qS, uS, (e, p)[o], u -> q (in place, with the convex
-    // combination), up buffer (becomes u^{n+1}), (e, p)[c]
     fill_common(ev, a);
     a.t_src = t + dt;
     a.t_inv = t + dt;
@@ -467,6 +469,19 @@ int rk2_step_t(vah_event *ev, double t, double dt) {
     a.pin = (const S *)ev->ep[o][1];
     a.eout = (S *)ev->ep[c][0];
     a.pout = (S *)ev->ep[c][1];
+}
+
+template <typename S>
+int rk2_step_t(vah_event *ev, double t, double dt) {
+    const int c = ev->cur;
+    if (ev->validity)  // the diagnostics read P_L, pi, Pi as they are at the start of the step
+        for (int n = VAH_F_PL; n < ev->nq; ++n)
+            VAH_TRY(cudaMemcpyAsync(ev->vq[n], ev->q[n], ev->ncell * sizeof(S), cudaMemcpyDeviceToDevice, ev->stream));
+    StageArgs<S> a;
+    stage1_args(ev, t, dt, a);
+    int rc = timed_launch(ev, a);
+    if (rc != VAH_OK) return rc;
+    stage2_args(ev, t, dt, a);
     rc = timed_launch(ev, a);
     if (rc != VAH_OK || !ev->validity) return rc;
     ValidityArgs<S> v;
@@ -714,6 +729,110 @@ int step_host_fp32(vah_event *ev, double t, double dt, double *const *fields) {
     return vah_event_sync(ev);
 }
 
+// Slab boundaries along eta for the overlapped host-buffer step: nz / thick
+// slabs (at least one) of as equal a thickness as nz allows, each of at least
+// `thick` >= 2 planes. (Thinner first and last slabs shorten the pipeline's
+// fill and drain but make more, smaller copies, which cost more than they
+// save on PCIe: measured on the 121x121x81 event.)
+std::vector<int> slab_bounds(int nz, int thick) {
+    thick = std::max(2, thick);
+    const int n = std::max(1, nz / thick);
+    std::vector<int> b = {0};
+    for (int m = 0; m < n; ++m) b.push_back(b.back() + nz / n + (m < nz % n ? 1 : 0));
+    return b;
+}
+
+// Host-buffer step (FP64 storage, face/cell split) with its copies
+// overlapped: the lattice is cut into slabs of planes along eta; the
+// host-to-device copy of later slabs, the stages of earlier ones and the
+// device-to-host copy of finished ones run on three streams. Slab m (interior
+// planes [lo, hi)) may start stage 1 once the input planes up to hi + 2
+// (ghosted) are on the device; its stage 2 follows stage 1 of slab m + 1
+// (which writes the stage-1 planes hi, hi + 1 that it reads); stage 1 of slab
+// m + 1 runs before stage 2 of slab m overwrites q, e and p in place under it.
+// Host planes are read (copy-in) before they are written back (copy-out):
+// each copy-out covers planes that the copy-ins before the slab's stage 1
+// have read. One compute stream keeps the face buffers' reuse in order.
+int step_host_pipelined(vah_event *ev, double t, double dt, double *const *fields, int thick) {
+    const int nz = ev->lat.nz;
+    const std::vector<int> bound = slab_bounds(nz, thick);
+    const int nslab = (int)bound.size() - 1;
+    const size_t pbytes = (size_t)ev->ncx * ev->ncy * sizeof(double);
+    if (!ev->s_in) VAH_TRY(cudaStreamCreateWithFlags(&ev->s_in, cudaStreamNonBlocking));
+    if (!ev->s_out) VAH_TRY(cudaStreamCreateWithFlags(&ev->s_out, cudaStreamNonBlocking));
+    while (ev->pev.size() < (size_t)(2 * nslab + 2)) {
+        cudaEvent_t e;
+        VAH_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ev->pev.push_back(e);
+    }
+    cudaEvent_t start = ev->pev[0], end = ev->pev[1], *in_ready = &ev->pev[2], *done = &ev->pev[2 + nslab];
+    // device buffers by field id: what the step reads, and what holds the field after it
+    void *din[VAH_NUM_FIELDS], *dout[VAH_NUM_FIELDS];
+    for (int id = 0; id < VAH_NUM_FIELDS; ++id) din[id] = dout[id] = fields[id] ? field_ptr(ev, id) : nullptr;
+    for (int m = 0; m < 4; ++m) {  // stage 2 writes u^{n+1} into the up buffer; u^n becomes up
+        if (fields[VAH_F_UT + m]) dout[VAH_F_UT + m] = ev->up[m];
+        if (fields[VAH_F_UPT + m]) dout[VAH_F_UPT + m] = ev->u[m];
+    }
+    auto copy_planes = [&](bool to_device, size_t p0, size_t p1, cudaStream_t s) -> int {
+        if (p1 <= p0) return VAH_OK;
+        for (int id = 0; id < VAH_NUM_FIELDS; ++id) {
+            if (!din[id]) continue;
+            char *h = (char *)fields[id] + p0 * pbytes;
+            if (to_device)
+                VAH_TRY(cudaMemcpyAsync((char *)din[id] + p0 * pbytes, h, (p1 - p0) * pbytes, cudaMemcpyHostToDevice, s));
+            else
+                VAH_TRY(cudaMemcpyAsync(h, (char *)dout[id] + p0 * pbytes, (p1 - p0) * pbytes, cudaMemcpyDeviceToHost, s));
+        }
+        return VAH_OK;
+    };
+    StageArgs<double> a1, a2;
+    stage1_args(ev, t, dt, a1);
+    stage2_args(ev, t, dt, a2);
+    const bool exact = ev->opt.flux == VAH_FLUX_PER_CELL;
+    VAH_TRY(cudaEventRecord(start, ev->stream));  // after the work queued before this step
+    VAH_TRY(cudaStreamWaitEvent(ev->s_in, start, 0));
+    VAH_TRY(cudaStreamWaitEvent(ev->s_out, start, 0));
+    size_t loaded = 0;  // ghosted planes [0, loaded) queued for copy-in
+    int rc = VAH_OK;
+    for (int m = 0; m <= nslab && rc == VAH_OK; ++m) {
+        if (m < nslab) {
+            const int hi = bound[m + 1];
+            const size_t need = m == nslab - 1 ? (size_t)nz + 4 : (size_t)hi + 4;
+            rc = copy_planes(true, loaded, need, ev->s_in);
+            if (rc != VAH_OK) break;
+            loaded = need;
+            VAH_TRY(cudaEventRecord(in_ready[m], ev->s_in));
+            VAH_TRY(cudaStreamWaitEvent(ev->stream, in_ready[m], 0));
+            a1.k0 = bound[m];
+            a1.k1 = hi;
+            VAH_TRY(vah::launch_stage_split<double>(a1, ev->opt.physics, exact, ev->split, ev->stream));
+        }
+        if (m >= 1) {
+            const int k = m - 1, lo = bound[k], hi = bound[k + 1];
+            a2.k0 = lo;
+            a2.k1 = hi;
+            VAH_TRY(vah::launch_stage_split<double>(a2, ev->opt.physics, exact, ev->split, ev->stream));
+            VAH_TRY(cudaEventRecord(done[k], ev->stream));
+            VAH_TRY(cudaStreamWaitEvent(ev->s_out, done[k], 0));
+            const size_t p0 = k == 0 ? 0 : (size_t)lo + 2, p1 = k == nslab - 1 ? (size_t)nz + 4 : (size_t)hi + 2;
+            rc = copy_planes(false, p0, p1, ev->s_out);
+        }
+    }
+    // join the copy streams back into the event's stream, also on an error
+    if (cudaEventRecord(end, ev->s_out) == cudaSuccess) cudaStreamWaitEvent(ev->stream, end, 0);
+    if (cudaEventRecord(end, ev->s_in) == cudaSuccess) cudaStreamWaitEvent(ev->stream, end, 0);
+    if (rc != VAH_OK) return rc;
+    for (int m = 0; m < 4; ++m) {  // as vah_rk2_step
+        void *tmp = ev->u[m];
+        ev->u[m] = ev->up[m];
+        ev->up[m] = tmp;
+    }
+    ev->steps++;
+    ev->last_t = t + dt;
+    ev->last_dt = dt;
+    return vah_event_sync(ev);
+}
+
 }  // namespace
 
 extern "C" int vah_rk2_step_host(vah_event *ev, double t, double dt, double *const *fields) {
@@ -721,6 +840,18 @@ extern "C" int vah_rk2_step_host(vah_event *ev, double t, double dt, double *con
     VAH_TRY(cudaSetDevice(ev->opt.device));
     int rc;
     if (ev->elem != sizeof(double)) return step_host_fp32(ev, t, dt, fields);
+    // overlapped copies where the lattice has enough planes along eta (at
+    // least 3 slabs); slab thickness from VAH_HOST_SLAB_PLANES (>= 2) when
+    // set, else nz / 6 (6 slabs: the best of 3 to 40 on the 121x121x81 event)
+    static const int slab_env = [] {
+        const char *v = getenv("VAH_HOST_SLAB_PLANES");
+        return v ? atoi(v) : 0;
+    }();
+    const int slab = slab_env >= 2 ? slab_env : std::max(2, ev->lat.nz / 6);
+    if (ev->opt.flux != VAH_FLUX_PER_CELL_FUSED && !ev->validity && ev->lat.nz >= 3 * slab) {
+        if (!(dt > 0) || !(t > 0)) return VAH_ERR_ARG;
+        return step_host_pipelined(ev, t, dt, fields, slab);
+    }
     const size_t bytes = ev->ncell * sizeof(double);
     // all copies are queued on the event's stream; one synchronisation at the end
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {

@@ -61,6 +61,8 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
     a.nx = d.nx;
     a.ny = d.ny;
     a.nz = d.nz;
+    a.k0 = 0;
+    a.k1 = d.nz;
     a.ncx = d.ncx;
     a.ncy = d.ncy;
     a.plane = d.plane;

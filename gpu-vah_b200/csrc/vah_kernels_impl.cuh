@@ -31,17 +31,18 @@ __global__ void __launch_bounds__(kBX *kBY) stage_kernel(const StageArgs<S> a) {
     stage_cell<S, PHYS, IS3D>(a, i + 2, j + 2, k + 2);
 }
 
-// Faces at +1/2 of the ghosted cells along DIR that bound an interior cell:
-// left cell index 1 .. n along DIR (ghost layer 1 included), interior across.
+// Faces at +1/2 of the ghosted cells along DIR that bound an interior cell
+// of the planes [k0, k1): left cell index 1 .. n along DIR (ghost layer 1
+// included), interior across.
 template <typename S, int PHYS, int DIR, bool EXACT, int MINB>
 __global__ void __launch_bounds__(kSplitThreads, MINB) face_kernel(const StageArgs<S> a) {
     const int ext0 = DIR == 0 ? a.nx + 1 : a.nx;
     const int ext1 = DIR == 1 ? a.ny + 1 : a.ny;
-    const int ext2 = DIR == 2 ? a.nz + 1 : a.nz;
+    const int ext2 = DIR == 2 ? a.k1 - a.k0 + 1 : a.k1 - a.k0;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= ext0 || r >= ext1 * ext2) return;
-    const int j = r % ext1, k = r / ext1;
+    const int j = r % ext1, k = r / ext1 + a.k0;
     const int gi = i + (DIR == 0 ? 1 : 2), gj = j + (DIR == 1 ? 1 : 2), gk = k + (DIR == 2 ? 1 : 2);
     const long long st = DIR == 0 ? 1 : (DIR == 1 ? (long long)a.ncx : a.plane);
     const long long s = gi + (long long)a.ncx * gj + a.plane * gk;
@@ -56,8 +57,8 @@ template <typename S, int PHYS, bool IS3D, bool EXACT, int MINB>
 __global__ void __launch_bounds__(kSplitThreads, MINB) cell_kernel(const StageArgs<S> a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= a.nx || r >= a.ny * a.nz) return;
-    const int j = r % a.ny, k = r / a.ny;
+    if (i >= a.nx || r >= a.ny * (a.k1 - a.k0)) return;
+    const int j = r % a.ny, k = r / a.ny + a.k0;
     cell_compute<S, PHYS, IS3D, EXACT>(a, i + 2, j + 2, k + 2);
 }
 
@@ -146,7 +147,7 @@ cudaError_t stage_dispatch(const StageArgs<S> &a, cudaStream_t stream) {
 template <typename S, int PHYS, bool EXACT, int DIR>
 cudaError_t face_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t stream) {
     const int ext0 = DIR == 0 ? a.nx + 1 : a.nx;
-    const int rows = (DIR == 1 ? a.ny + 1 : a.ny) * (DIR == 2 ? a.nz + 1 : a.nz);
+    const int rows = (DIR == 1 ? a.ny + 1 : a.ny) * (DIR == 2 ? a.k1 - a.k0 + 1 : a.k1 - a.k0);
     const dim3 block(c.bx, c.by), grid((ext0 + c.bx - 1) / c.bx, (rows + c.by - 1) / c.by);
     switch (c.minb) {
     case 3: face_kernel<S, PHYS, DIR, EXACT, 3><<<grid, block, 0, stream>>>(a); break;
@@ -159,7 +160,7 @@ cudaError_t face_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t
 
 template <typename S, int PHYS, bool EXACT, bool IS3D>
 cudaError_t cell_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t stream) {
-    const dim3 block(c.bx, c.by), grid((a.nx + c.bx - 1) / c.bx, (a.ny * a.nz + c.by - 1) / c.by);
+    const dim3 block(c.bx, c.by), grid((a.nx + c.bx - 1) / c.bx, (a.ny * (a.k1 - a.k0) + c.by - 1) / c.by);
     switch (c.minb) {
     case 2: cell_kernel<S, PHYS, IS3D, EXACT, 2><<<grid, block, 0, stream>>>(a); break;
     case 3: cell_kernel<S, PHYS, IS3D, EXACT, 3><<<grid, block, 0, stream>>>(a); break;
@@ -171,6 +172,8 @@ cudaError_t cell_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t
 
 template <typename S, int PHYS, bool EXACT>
 cudaError_t split_kind_dispatch(const StageArgs<S> &a, int kind, const KindConfig &c, cudaStream_t stream) {
+    if (a.k0 < 0 || a.k1 > a.nz || a.k0 > a.k1) return cudaErrorInvalidValue;
+    if (a.k0 == a.k1) return cudaSuccess;  // no planes
     switch (kind) {
     case kFaceX: return face_launch<S, PHYS, EXACT, 0>(a, c, stream);
     case kFaceY: return face_launch<S, PHYS, EXACT, 1>(a, c, stream);

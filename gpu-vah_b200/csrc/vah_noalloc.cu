@@ -88,6 +88,8 @@ extern "C" int vah_stage_noalloc(const vah_lattice *lat, double eta_over_s, int 
     a.nx = lat->nx;
     a.ny = lat->ny;
     a.nz = lat->nz;
+    a.k0 = 0;
+    a.k1 = lat->nz;
     a.ncx = lat->nx + 4;
     a.ncy = lat->ny + 4;
     a.plane = (long long)a.ncx * a.ncy;

@@ -19,6 +19,7 @@ namespace vah {
 template <typename S>
 struct StageArgs {
     int nx, ny, nz;
+    int k0, k1;       // face/cell split launches: the interior planes [k0, k1) they update (all: 0, nz)
     int ncx, ncy;
     long long plane;  // ncx * ncy
     double t_src;     // time of the Euler step (stage 1: t, stage 2: t + dt)

@@ -82,6 +82,7 @@ void stage(HostEvent *h, const vah::StageArgs<double> &a) {
 void common(HostEvent *h, vah::StageArgs<double> &a) {
     std::memset(&a, 0, sizeof(a));
     a.nx = h->nx; a.ny = h->ny; a.nz = h->nz; a.ncx = h->ncx; a.ncy = h->ncy;
+    a.k0 = 0; a.k1 = h->nz;
     a.plane = (long long)h->ncx * h->ncy;
     a.dx = h->dx; a.dy = h->dy; a.dz = h->dz; a.etabar = h->etabar;
     a.eos = h->eos;
