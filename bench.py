@@ -249,6 +249,26 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# FP64 vector peak: 64 DFMA per cycle per SM (the profiler's peak_sustained
+# for sm__sass_thread_inst_executed_op_dfma_pred_on) x 2 FLOP x 148 SMs x 1965 MHz.
+FP64_PEAK_TFLOPS = 64 * 2 * 148 * 1.965e9 / 1e12
+
+
+def fp64_roofline(cells, flux, precision, stage_s):
+    """FP64 FLOP/s of one RK stage against the FP64 vector peak, from the
+    FLOP count per cell and stage in the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "split_stage_dram.json")
+    if flux != "per_cell" or not os.path.exists(path) or not stage_s:
+        return None
+    with open(path) as f:
+        per = json.load(f).get("fp64_flop_per_cell_per_stage", {}).get(precision)
+    if not per:
+        return None
+    achieved = per * cells / stage_s / 1e12
+    return {"achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS,
+            "flop_per_cell_update": 2 * per, "peak_kind": "nominal FP64 vector peak (64 DFMA/cycle/SM at 1965 MHz)"}
+
+
 def traffic_per_launch(cells, flux, precision):
     """DRAM bytes of one RK stage (its launches) from the committed ncu
     summaries (bytes per interior cell, scaled to this event), or None."""
@@ -552,7 +572,8 @@ def run_vah(args, rank, world, dist):
                          "algorithmic_bytes_per_cell_update": bpc,
                          "kernel": ("stage_kernel (one fused RK stage)" if args.flux == "fused"
                                     else "one RK stage: face_kernel x3 + cell_kernel") + ", average over the two stages",
-                         "avg_stage_ms": 1000 * avg_launch_s},
+                         "avg_stage_ms": 1000 * avg_launch_s,
+                         "fp64": fp64_roofline(cells, args.flux, args.precision, avg_launch_s)},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
                     "path": "vah_rk2_step_host (pinned host state in, one step, state out)"},
