@@ -22,10 +22,21 @@ namespace {
 
 constexpr int kBX = 32, kBY = 4;  // fused stage kernel shape
 
+// Row blocks beyond the grid's y limit (65535) continue along z.
+constexpr unsigned kMaxGridY = 65535;
+
+__device__ __forceinline__ int row_block() { return (int)(blockIdx.z * gridDim.y + blockIdx.y); }
+
+dim3 row_grid(long long cols, long long rows, int bx, int by) {
+    const unsigned gy = (unsigned)((rows + by - 1) / by);
+    const unsigned gz = (gy + kMaxGridY - 1) / kMaxGridY;
+    return dim3((unsigned)((cols + bx - 1) / bx), gz > 1 ? kMaxGridY : gy, gz > 1 ? gz : 1);
+}
+
 template <typename S, int PHYS, bool IS3D>
 __global__ void __launch_bounds__(kBX *kBY) stage_kernel(const StageArgs<S> a) {
     const int i = blockIdx.x * kBX + threadIdx.x;
-    const int r = blockIdx.y * kBY + threadIdx.y;  // row index over (j, k)
+    const int r = row_block() * kBY + threadIdx.y;  // row index over (j, k)
     if (i >= a.nx || r >= a.ny * a.nz) return;
     const int j = r % a.ny, k = r / a.ny;
     stage_cell<S, PHYS, IS3D>(a, i + 2, j + 2, k + 2);
@@ -40,7 +51,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) face_kernel(const StageAr
     const int ext1 = DIR == 1 ? a.ny + 1 : a.ny;
     const int ext2 = DIR == 2 ? a.k1 - a.k0 + 1 : a.k1 - a.k0;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    const int r = row_block() * blockDim.y + threadIdx.y;
     if (i >= ext0 || r >= ext1 * ext2) return;
     const int j = r % ext1, k = r / ext1 + a.k0;
     const int gi = i + (DIR == 0 ? 1 : 2), gj = j + (DIR == 1 ? 1 : 2), gk = k + (DIR == 2 ? 1 : 2);
@@ -56,7 +67,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) face_kernel(const StageAr
 template <typename S, int PHYS, bool IS3D, bool EXACT, int MINB>
 __global__ void __launch_bounds__(kSplitThreads, MINB) cell_kernel(const StageArgs<S> a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    const int r = row_block() * blockDim.y + threadIdx.y;
     if (i >= a.nx || r >= a.ny * (a.k1 - a.k0)) return;
     const int j = r % a.ny, k = r / a.ny + a.k0;
     cell_compute<S, PHYS, IS3D, EXACT>(a, i + 2, j + 2, k + 2);
@@ -135,7 +146,7 @@ __global__ void ghost_kernel(const FieldSet<S> f, int nx, int ny, int nz, int pa
 template <typename S, int PHYS>
 cudaError_t stage_dispatch(const StageArgs<S> &a, cudaStream_t stream) {
     dim3 block(kBX, kBY);
-    dim3 grid((a.nx + kBX - 1) / kBX, (a.ny * a.nz + kBY - 1) / kBY);
+    const dim3 grid = row_grid(a.nx, (long long)a.ny * a.nz, kBX, kBY);
     if (a.nz > 1)
         stage_kernel<S, PHYS, true><<<grid, block, 0, stream>>>(a);
     else
@@ -148,7 +159,7 @@ template <typename S, int PHYS, bool EXACT, int DIR>
 cudaError_t face_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t stream) {
     const int ext0 = DIR == 0 ? a.nx + 1 : a.nx;
     const int rows = (DIR == 1 ? a.ny + 1 : a.ny) * (DIR == 2 ? a.k1 - a.k0 + 1 : a.k1 - a.k0);
-    const dim3 block(c.bx, c.by), grid((ext0 + c.bx - 1) / c.bx, (rows + c.by - 1) / c.by);
+    const dim3 block(c.bx, c.by), grid = row_grid(ext0, rows, c.bx, c.by);
     switch (c.minb) {
     case 3: face_kernel<S, PHYS, DIR, EXACT, 3><<<grid, block, 0, stream>>>(a); break;
     case 4: face_kernel<S, PHYS, DIR, EXACT, 4><<<grid, block, 0, stream>>>(a); break;
@@ -160,7 +171,7 @@ cudaError_t face_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t
 
 template <typename S, int PHYS, bool EXACT, bool IS3D>
 cudaError_t cell_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t stream) {
-    const dim3 block(c.bx, c.by), grid((a.nx + c.bx - 1) / c.bx, (a.ny * (a.k1 - a.k0) + c.by - 1) / c.by);
+    const dim3 block(c.bx, c.by), grid = row_grid(a.nx, (long long)a.ny * (a.k1 - a.k0), c.bx, c.by);
     switch (c.minb) {
     case 2: cell_kernel<S, PHYS, IS3D, EXACT, 2><<<grid, block, 0, stream>>>(a); break;
     case 3: cell_kernel<S, PHYS, IS3D, EXACT, 3><<<grid, block, 0, stream>>>(a); break;

@@ -161,6 +161,27 @@ def test_gpu_ideal_3d_matches_oracle():
     ev.close()
 
 
+@pytest.mark.parametrize("flux", [0, 2], ids=["split", "fused"])
+def test_gpu_tall_lattice_beyond_the_grid_y_limit(flux):
+    """1 x 512 x 512 cells: 262,144 rows of (j, k), more row blocks than a
+    grid's y dimension holds (65,535 blocks of 4 rows); the launches continue
+    along z. Two steps against the oracle."""
+    g = V.Grid(1, 512, 512, 0.2, 0.2, 0.2, 0.2, physics="ideal", eos="conformal")
+    f = V.smooth_initial_state(g, 0.5, flow=0.4)
+    o = V.Oracle(g)
+    V.load_state(o, f)
+    o.set_conserved(0.5, 1)
+    o.set_ghost_cells()
+    ev = V.Event(g, t0=0.5, flux=flux)
+    upload(ev, g, {fid: o.field(fid).copy() for fid in V.state_ids(g.physics)})
+    o.run(0.5, 0.02, 2)
+    ev.run(0.5, 0.02, 2)
+    ev.sync()
+    for fid in KEY_FIELDS:
+        assert rel_err(g.interior(o.field(fid)), g.interior(ev.get_field(fid)), 1e-12) < 1e-11, fid
+    ev.close()
+
+
 def test_gpu_host_buffer_step_matches_device_step():
     g, e2 = conformal_workload(21, 19)
     ev = V.Event(g, t0=0.5)
