@@ -208,6 +208,9 @@ VAH_HD double approx_derivative(double x, double y, double z) {
 // face, inverted from both neighbours' guesses, sets up each state once.
 struct InvSetup {
     double pl, bulk, m0, m1, m2, m3, F, x, mbt, bT, bL, b, c0;
+    // g(v) = bL + b (0.5 (e(v) - pl) + 1.5 Pi) with e(v) = c0 - v x mbt, expanded:
+    // g = G0 - G1 v, and g - 0.5 b bT v = G0 - 2 G1 v (the derivative's factor)
+    double G0, G1;
 };
 
 template <int PHYS>
@@ -243,6 +246,8 @@ VAH_HD void invert_setup(double t, const double *q, InvSetup &s) {
     s.bL = x * x * m0 - Ft2 * pl;
     s.b = x * x + Ft2;
     s.c0 = m0 - t * Ft * m3;
+    s.G0 = s.bL + s.b * (0.5 * (s.c0 - pl) + 1.5 * bulk);
+    s.G1 = 0.5 * s.b * s.bT;
 }
 
 // The Newton correction f / fp. On the device: the hardware reciprocal
@@ -267,19 +272,19 @@ VAH_HD double newton_correction(double f, double fp) {
 // Newton iteration for u_T from the guess uT0 (EnergyMomentumTensor.cpp:30-72).
 // Returns 0 with the root in uT, or 1 when the reference falls back.
 VAH_HD int newton_uT(const InvSetup &s, double uT0, double &uT) {
-    const double x = s.x, mbt = s.mbt, bT = s.bT, bL = s.bL, b = s.b, c0 = s.c0, pl = s.pl, bulk = s.bulk;
+    const double x = s.x, mbt = s.mbt, bT = s.bT, c0 = s.c0, G0 = s.G0, G1 = s.G1;
     double w = uT0;
     uT = uT0;
     for (int it = 0; it < 10000; ++it) {
         const double w2 = 1 + w * w;
         const double r = rsqrt_d(w2);
         const double v = w * r;
-        const double e = c0 - v * x * mbt;
+        const double e = c0 - v * x * mbt;  // the reference's energy, for its exit test
         if (e < 0.0) return 1;
-        const double g = bL + b * (0.5 * (e - pl) + 1.5 * bulk);
+        const double g = G0 - G1 * v;  // bL + b (0.5 (e - pl) + 1.5 Pi), one operation after v
         const double r3 = r * r * r;
         const double f = v * g - bT;
-        double fp = r3 * g + v * b * (0.5 * (-bT * r3));
+        double fp = r3 * (G0 - 2 * G1 * v);  // r3 g + v b (0.5 (-bT r3))
         if (fabs(fp) == 0.0) fp = 1.e-16;
         const double next = w - newton_correction(f, fp);
         uT = next;
@@ -298,11 +303,11 @@ VAH_HD int newton_step(const InvSetup &s, double w, double &next) {
     const double w2 = 1 + w * w;
     const double r = rsqrt_d(w2);
     const double v = w * r;
-    const double e = s.c0 - v * s.x * s.mbt;
-    const double g = s.bL + s.b * (0.5 * (e - s.pl) + 1.5 * s.bulk);
+    const double e = s.c0 - v * s.x * s.mbt;  // the reference's energy, for its exit test
+    const double g = s.G0 - s.G1 * v;          // bL + b (0.5 (e - pl) + 1.5 Pi), one operation after v
     const double r3 = r * r * r;
     const double f = v * g - s.bT;
-    double fp = r3 * g + v * s.b * (0.5 * (-s.bT * r3));
+    double fp = r3 * (s.G0 - 2 * s.G1 * v);   // r3 g + v b (0.5 (-bT r3))
     if (fabs(fp) == 0.0) fp = 1.e-16;
     next = w - newton_correction(f, fp);
     if (e < 0.0) return 1;
