@@ -6,6 +6,7 @@
 // No call ever exits or traps; failures come back as status codes.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
@@ -178,6 +179,54 @@ int timed_launch(vah_event *ev, const StageArgs<S> &a) {
 }  // namespace
 
 extern "C" const char *vah_version(void) { return "vah-b200 0.1 (sm_100a)"; }
+
+namespace {
+
+// Per input: relative error of the Newton correction's reciprocal and of
+// rsqrt_d against CUDA's IEEE-rounded operations.
+__global__ void math_check_kernel(const double *x, double *err, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = x[i];
+        const double r_ref = __drcp_rn(v);
+        err[2 * i] = fabs(vah::newton_correction(1.0, v) - r_ref) / fabs(r_ref);
+        const double a = fabs(v), s_ref = 1.0 / __dsqrt_rn(a);
+        err[2 * i + 1] = fabs(vah::rsqrt_d(a) - s_ref) / s_ref;
+    }
+}
+
+}  // namespace
+
+extern "C" int vah_math_check(int device, double lo, double hi, int n, double *max_rel_rcp, double *max_rel_rsqrt) {
+    if (!max_rel_rcp || !max_rel_rsqrt || n < 2 || !(lo > 0) || !(hi > lo)) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(device));
+    std::vector<double> x(n), err(2 * (size_t)n);
+    const double l0 = std::log(lo), l1 = std::log(hi);
+    for (int i = 0; i < n; ++i) x[i] = (i & 1 ? -1.0 : 1.0) * std::exp(l0 + (l1 - l0) * i / (n - 1));
+    double *d_x = nullptr, *d_err = nullptr;
+    int rc = VAH_OK;
+    if (cudaMalloc((void **)&d_x, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void **)&d_err, 2 * (size_t)n * sizeof(double)) != cudaSuccess)
+        rc = VAH_ERR_NOMEM;
+    if (rc == VAH_OK && cudaMemcpy(d_x, x.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = VAH_ERR_CUDA;
+    if (rc == VAH_OK) {
+        math_check_kernel<<<148 * 4, 256>>>(d_x, d_err, n);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpy(err.data(), d_err, err.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = VAH_ERR_CUDA;
+    }
+    cudaFree(d_x);
+    cudaFree(d_err);
+    if (rc != VAH_OK) return rc;
+    double m0 = 0, m1 = 0;
+    for (int i = 0; i < n; ++i) {  // a NaN error counts as infinite
+        m0 = std::max(m0, err[2 * i] == err[2 * i] ? err[2 * i] : INFINITY);
+        m1 = std::max(m1, err[2 * i + 1] == err[2 * i + 1] ? err[2 * i + 1] : INFINITY);
+    }
+    *max_rel_rcp = m0;
+    *max_rel_rsqrt = m1;
+    return VAH_OK;
+}
 
 extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, const vah_options *opt,
                                 const double *eos_table, vah_event **out) {

@@ -446,6 +446,15 @@ int vah_stage_noalloc(const vah_lattice *lat, double eta_over_s, int physics, in
                       const double *d_eos_table, int stage, double t, double dt, const vah_stage_buffers *buf,
                       void *stream, long long *counts_out);
 
+/* Accuracy check of the step's two hand-written device operations: the
+ * Newton correction's reciprocal (hardware estimate + one Newton-Raphson
+ * step) and 1/sqrt (hardware estimate + two steps), against CUDA's
+ * IEEE-rounded reciprocal and square root, on n log-spaced inputs in
+ * [lo, hi] (alternating sign for the reciprocal). Writes the largest relative
+ * errors. No counterpart in the reference, which divides and takes square
+ * roots in IEEE arithmetic on the CPU. */
+int vah_math_check(int device, double lo, double hi, int n, double *max_rel_rcp, double *max_rel_rsqrt);
+
 /* Library version string. */
 const char *vah_version(void);
 
