@@ -774,18 +774,35 @@ VAH_HD void regulate(double t, double &e, double &p, double *q, const double *u,
     const double spipi = sqrt(fabs(pipi));
     double rho = spipi / sTrsTrs;
     const double den = spipi;
-    const double cand[9] = {(pitt - pixx - piyy - pinn * t2) / den,
-                            (-pitn * t2 * un + pitt * ut - pitx * ux - pity * uy) / den,
-                            (-pixn * t2 * un + pitx * ut - pixx * ux - pixy * uy) / den,
-                            (-piyn * t2 * un + pity * ut - pixy * ux - piyy * uy) / den,
-                            (-pinn * t2 * un + pitn * ut - pixn * ux - piyn * uy) / den,
-                            (z0 * pitt - t2 * z3 * pitn) / den,
-                            (z0 * pitx - t2 * z3 * pixn) / den,
-                            (z0 * pity - t2 * z3 * piyn) / den,
-                            (z0 * pitn - t2 * z3 * pinn) / den};
+    const double num[9] = {pitt - pixx - piyy - pinn * t2,
+                           -pitn * t2 * un + pitt * ut - pitx * ux - pity * uy,
+                           -pixn * t2 * un + pitx * ut - pixx * ux - pixy * uy,
+                           -piyn * t2 * un + pity * ut - pixy * ux - piyy * uy,
+                           -pinn * t2 * un + pitn * ut - pixn * ux - piyn * uy,
+                           z0 * pitt - t2 * z3 * pitn,
+                           z0 * pitx - t2 * z3 * pixn,
+                           z0 * pity - t2 * z3 * piyn,
+                           z0 * pitn - t2 * z3 * pinn};
+    double cand[9];
+    if (maps) {  // every ratio is reported
 #pragma unroll
-    for (int m = 0; m < 9; ++m)
-        if (cand[m] > rho) rho = cand[m];
+        for (int m = 0; m < 9; ++m) {
+            cand[m] = num[m] / den;
+            if (cand[m] > rho) rho = cand[m];
+        }
+    } else {
+        // rho = max(rho, num[m] / den): den = sqrt(|pi.pi|) >= 0 and a rounded
+        // division by it is monotone, so the largest ratio is the largest
+        // numerator divided once -- the same value bit for bit, NaN ratios
+        // (0/0, NaN numerators) ignored as the comparisons ignore them, and
+        // den = 0 giving +-inf as the nine quotients would.
+        double top = -INFINITY;
+#pragma unroll
+        for (int m = 0; m < 9; ++m)
+            if (num[m] > top) top = num[m];
+        const double c = top / den;
+        if (c > rho) rho = c;
+    }
     double fac = tanh(rho) / rho;
     if (rho < 1.e-7) fac = 1.0;
 #pragma unroll
