@@ -299,7 +299,8 @@ VAH_HD int newton_uT(const InvSetup &s, double uT0, double &uT) {
         if (fabs(fp) == 0.0) fp = 1.e-16;
         const double next = w - newton_correction(f, fp);
         uT = next;
-        if (isnan(next) || isinf(next) || next < 0 || next > 9.0072e+15) return 1;
+        // NaN, +-inf, negative or above 9.0072e15 (one test: NaN fails both comparisons)
+        if (!(next >= 0.0 && next <= 9.0072e+15)) return 1;
         if (fabs(next - w) <= 1.e-7 * fabs(next)) return 0;
         w = next;
     }
@@ -322,7 +323,7 @@ VAH_HD int newton_step(const InvSetup &s, double w, double &next) {
     if (fabs(fp) == 0.0) fp = 1.e-16;
     next = w - newton_correction(f, fp);
     if (e < 0.0) return 1;
-    if (isnan(next) || isinf(next) || next < 0 || next > 9.0072e+15) return 1;
+    if (!(next >= 0.0 && next <= 9.0072e+15)) return 1;  // NaN, +-inf, negative or too large
     return fabs(next - w) <= 1.e-7 * fabs(next) ? 0 : 2;
 }
 
@@ -402,8 +403,8 @@ VAH_HD int face_velocity(const InvSetup &s, double ePrev, double uT0, int dir, d
     if (dir == 2) {
         vv = s.F;
     } else {
-        const double C = sqrt(1.0 + uT * uT);
-        vv = uT * (dir == 0 ? s.m1 : s.m2) * s.x / (s.mbt * C);
+        // uT m x / (mbt C), C = sqrt(1 + uT^2), with 1/C from rsqrt_d
+        vv = uT * (dir == 0 ? s.m1 : s.m2) * s.x * rsqrt_d(1.0 + uT * uT) / s.mbt;
     }
     *v = vv;
     return (isnan(vv) || isnan(s.c0)) ? 2 : 0;
@@ -423,8 +424,8 @@ VAH_HD int face_velocity_of(const InvSetup &s, double uT, int dir, double *v) {
     if (dir == 2) {
         vv = s.F;
     } else {
-        const double C = sqrt(1.0 + uT * uT);
-        vv = uT * (dir == 0 ? s.m1 : s.m2) * s.x / (s.mbt * C);
+        // uT m x / (mbt C), C = sqrt(1 + uT^2), with 1/C from rsqrt_d
+        vv = uT * (dir == 0 ? s.m1 : s.m2) * s.x * rsqrt_d(1.0 + uT * uT) / s.mbt;
     }
     *v = vv;
     return (isnan(vv) || isnan(s.c0)) ? 2 : 0;
@@ -480,6 +481,14 @@ VAH_HD void axis_sources(const double *d, int dir, double ucomp, double ut, doub
     }
 }
 
+// x / d for a constant d with its rounded reciprocal inv_d: the product and
+// one FMA correction (q + (x - q d) inv_d), within an ulp of the quotient
+// (usually the correctly rounded one), in three operations.
+VAH_HD double div_const(double x, double d, double inv_d) {
+    const double q = x * inv_d;
+    return fma(fma(-q, d, x), inv_d, q);
+}
+
 // ----------------------------------------------------------- cell sources --
 // Inputs of the local source terms at one cell: stage-input conserved values,
 // primitives, previous-stage velocity and central differences (q(+1)-q(-1))/(2h).
@@ -528,7 +537,7 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, doub
     const double Dux = -dux, Duy = -duy;
     const double Dun = -t2 * (dun + 2 * ut * un * inv_t);
     const double theta = ut * inv_t + dtut + dxux + dyuy + dnun;
-    const double th3 = theta / 3;
+    const double th3 = div_const(theta, 3.0, 1.0 / 3.0);
 
     const double stt = -t * ut * un2 + (dtut - ut * dut) + (ut2 - 1) * th3;
     const double stx = -(t * un2 * ux) * 0.5 + (dtux - dxut) * 0.5 - (ux * dut + ut * dux) * 0.5 + ut * ux * th3;
@@ -626,7 +635,7 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, doub
     const double zeta_zz = Rtilde * e - 3 * pl;
     const double zeta_zT = (Rtilde * e + pl) * 0.5;
     const double delta_pipi = (3 + Rgamma) * 0.5;
-    const double tau_pipi = 4 * delta_pipi / 3;  // SourceTerms.cpp:634, 1/2 -> 0
+    const double tau_pipi = div_const(4 * delta_pipi, 3.0, 1.0 / 3.0);  // SourceTerms.cpp:634, 1/2 -> 0
     const double lambda_pipi = Rgamma - 1;
     const double taupiInv = 0.2 * T / etabar;
 
@@ -648,7 +657,7 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, doub
         delta_lPi = g20 + g40;
         beta_PiPi = 1 - g20c;
         delta_PiPi = 0.5 * (1 + g20c);
-        lambda_Pipi = 3 * poly::G_G1(ap) / 5 * (0 - cs2);
+        lambda_Pipi = div_const(3 * poly::G_G1(ap), 5.0, 1.0 / 5.0) * (0 - cs2);
     }
 
     const double dPL = -(pl - p) * taupiInv + zeta_zz * zDzu - zeta_zT * thetaT - beta_lPi * Pi * zDzu -
@@ -731,9 +740,9 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, doub
         const double Rhat = poly::Rhat(ap);
         const double bb = 1.0 / 3.0 - cs2;
         const double tauPiInv = 15 * bb * bb * T / zeta_over_s(eos, T);
-        const double zeta_z = (Rhat - Rbar0) * e3p / 3;
-        const double zeta_T = -(Rbar0 + Rhat) * e3p / 6;
-        const double dPi = -((1 - Rbar0) * e3p / 3 + Pi) * tauPiInv - zeta_z * zDzu - zeta_T * thetaT -
+        const double zeta_z = div_const((Rhat - Rbar0) * e3p, 3.0, 1.0 / 3.0);
+        const double zeta_T = div_const(-(Rbar0 + Rhat) * e3p, 6.0, 1.0 / 6.0);
+        const double dPi = -(div_const((1 - Rbar0) * e3p, 3.0, 1.0 / 3.0) + Pi) * tauPiInv - zeta_z * zDzu - zeta_T * thetaT -
                            beta_PiPi * Pi * zDzu - delta_PiPi * Pi * thetaT + lambda_Pipi * psT;
         S[kSlotPi] = dPi * inv_ut + Pi * dkvk;
     }
