@@ -202,13 +202,15 @@ VAH_HD double zeta_over_s(const Eos &eos, double T) {
 // that sign times min(|l|, |c|, |r|), else 0. The same value bit for bit for
 // every y that is not NaN (checked exhaustively on edge values and on 5e7
 // random triples); a NaN y makes the caller's state NaN either way.
+// With l = 1.1 (y - x) and r = 1.1 (z - y), min(|l|, |r|) is 1.1 min(|y - x|,
+// |z - y|) rounded once (rounding is monotone), and l, r have the signs of
+// y - x, z - y.
 VAH_HD double approx_derivative(double x, double y, double z) {
-    const double l = 1.1 * (y - x);
+    const double dl = y - x, dr = z - y;
     const double c = (z - x) * 0.5;
-    const double r = 1.1 * (z - y);
-    const double m = fmin(fmin(fabs(l), fabs(c)), fabs(r));
-    const bool neg = l < 0.0;
-    return neg == (r < 0.0) ? (neg ? -m : m) : 0.0;
+    const double m = fmin(1.1 * fmin(fabs(dl), fabs(dr)), fabs(c));
+    const bool neg = dl < 0.0;
+    return neg == (dr < 0.0) ? (neg ? -m : m) : 0.0;
 }
 
 // ------------------------------------------------------------- inversion --
@@ -445,7 +447,7 @@ VAH_HD int face_flux_setup(const InvSetup &sR, const InvSetup &sL, const double 
     const int stL = nL != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sL, uL, dir, &vL);
     const double a = fmax(fabs(vL), fabs(vR));
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) H[n] = 0.5 * (vR * qR[n] + vL * qL[n] - a * (qR[n] - qL[n]));
+    for (int n = 0; n < NQ; ++n) H[n] = 0.5 * ((vR - a) * qR[n] + (vL + a) * qL[n]);  // vR qR + vL qL - a (qR - qL)
     return (stR != 0) + (stL != 0) + ((stR == 2 || stL == 2) ? 256 : 0);
 }
 
