@@ -491,6 +491,7 @@ void stage1_args(const vah_event *ev, double t, double dt, StageArgs<S> &a) {
     a.pin = (const S *)ev->ep[c][1];
     a.eout = (S *)ev->ep[o][0];
     a.pout = (S *)ev->ep[o][1];
+    finish_args(a);
 }
 
 // Stage 2: qS, uS, (e, p)[o], u -> q (in place, with the convex
@@ -518,6 +519,7 @@ void stage2_args(const vah_event *ev, double t, double dt, StageArgs<S> &a) {
     a.pin = (const S *)ev->ep[o][1];
     a.eout = (S *)ev->ep[c][0];
     a.pout = (S *)ev->ep[c][1];
+    finish_args(a);
 }
 
 template <typename S>

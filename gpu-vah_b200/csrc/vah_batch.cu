@@ -103,6 +103,7 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
             a.H[k][n] = d.H[k][n];
             a.HR[k][n] = d.HR[k][n];
         }
+    finish_args(a);
 }
 
 template <typename S, int PHYS, int KIND, bool EXACT, int MINB>

@@ -129,6 +129,7 @@ extern "C" int vah_stage_noalloc(const vah_lattice *lat, double eta_over_s, int 
             a.HR[d][n] = faces + ((size_t)(d * nq + n) * 2 + 1) * ncell;
         }
 
+    vah::finish_args(a);
     if (cudaMemsetAsync(base, 0, kCounterBytes, s) != cudaSuccess) return VAH_ERR_CUDA;
     if (vah::launch_stage_split<double>(a, physics, true, s) != cudaSuccess) return VAH_ERR_CUDA;
     if (counts_out) {

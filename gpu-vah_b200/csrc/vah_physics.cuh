@@ -446,8 +446,10 @@ VAH_HD int face_flux_setup(const InvSetup &sR, const InvSetup &sL, const double 
     const int stR = nR != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sR, uR, dir, &vR);
     const int stL = nL != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sL, uL, dir, &vL);
     const double a = fmax(fabs(vL), fabs(vR));
+    // (vR qR + vL qL - a (qR - qL)) / 2 = wR qR + wL qL; the halving is exact
+    const double wR = 0.5 * (vR - a), wL = 0.5 * (vL + a);
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) H[n] = 0.5 * ((vR - a) * qR[n] + (vL + a) * qL[n]);  // vR qR + vL qL - a (qR - qL)
+    for (int n = 0; n < NQ; ++n) H[n] = wR * qR[n] + wL * qL[n];
     return (stR != 0) + (stL != 0) + ((stR == 2 || stL == 2) ? 256 : 0);
 }
 
@@ -503,10 +505,27 @@ struct CellGrad {
     double dxp, dyp, dnp, dxe, dye, dne, dxpl, dypl, dnpl;
 };
 
+// The sources' per-launch constants, formed once per launch with the same
+// operations as the per-cell expressions they stand for (bit-identical).
+struct StepConsts {
+    double t, dt, etabar, inv_t, inv_t2, inv_dt;
+};
+
+VAH_HD StepConsts step_consts(double t, double dt, double etabar) {
+    StepConsts k;
+    k.t = t;
+    k.dt = dt;
+    k.etabar = etabar;
+    k.inv_t = 1.0 / t;
+    k.inv_t2 = 1.0 / (t * t);
+    k.inv_dt = 1.0 / dt;
+    return k;
+}
+
 // Geometric and relaxation sources S[n] (SourceTerms.cpp:178-1044), W off.
 template <int PHYS>
-VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, double t, double dt, double etabar,
-                        double *S) {
+VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, const StepConsts &k, double *S) {
+    const double t = k.t, etabar = k.etabar;
     constexpr bool PIM = Phys<PHYS>::PIMUNU, BULK = Phys<PHYS>::BULK;
     const double ttt = Q[0], ttx = Q[1], tty = Q[2], ttn = Q[3], pl = Q[4];
     double pitt = 0, pitx = 0, pity = 0, pitn = 0, pixx = 0, pixy = 0, pixn = 0, piyy = 0, piyn = 0, pinn = 0,
@@ -522,15 +541,15 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, doub
     const double dyut = g.dyut, dyux = g.dyux, dyuy = g.dyuy, dyun = g.dyun;
     const double dnut = g.dnut, dnux = g.dnux, dnuy = g.dnuy, dnun = g.dnun;
 
-    const double inv_ut = 1.0 / ut, inv_t = 1.0 / t;
+    const double inv_ut = 1.0 / ut, inv_t = k.inv_t;
     const double vx = ux * inv_ut, vy = uy * inv_ut, vn = un * inv_ut;
     const double dkvk = (dxux - vx * dxut) * inv_ut + (dyuy - vy * dyut) * inv_ut + (dnun - vn * dnut) * inv_ut;
 
     const double t2 = t * t, t3 = t * t2, un2 = un * un, ut2 = ut * ut;
-    const double inv_t2 = 1.0 / t2;
+    const double inv_t2 = k.inv_t2;
 
     // velocity gradients (SourceTerms.cpp:301-334)
-    const double inv_dt = 1.0 / dt;
+    const double inv_dt = k.inv_dt;
     const double dtut = (ut - g.utp) * inv_dt, dtux = (ux - g.uxp) * inv_dt;
     const double dtuy = (uy - g.uyp) * inv_dt, dtun = (un - g.unp) * inv_dt;
     const double dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;

@@ -23,6 +23,9 @@ struct StageArgs {
     int ncx, ncy;
     long long plane;  // ncx * ncy
     double t_src;     // time of the Euler step (stage 1: t, stage 2: t + dt)
+    // derived per launch by finish_args: the sources' constants at t_src, dt / h and 1 / (2 h) per axis
+    StepConsts ksrc;
+    double c_h[3], inv2h[3];
     double t_inv;     // time of the inversion/regulator (t + dt)
     double dt, dx, dy, dz, etabar;
     int stage2;       // 1: convex combination with qavg before inversion
@@ -60,6 +63,18 @@ VAH_HD void count_add(unsigned long long *c, unsigned long long v) {
 #endif
 }
 
+// The launch constants derived from t_src, dt, etabar and the spacings; to be
+// called once the arguments are filled.
+template <typename S>
+VAH_HD void finish_args(StageArgs<S> &a) {
+    a.ksrc = step_consts(a.t_src, a.dt, a.etabar);
+    const double h[3] = {a.dx, a.dy, a.dz};
+    for (int d = 0; d < 3; ++d) {
+        a.c_h[d] = a.dt / h[d];
+        a.inv2h[d] = 1 / h[d] / 2;
+    }
+}
+
 template <typename S>
 VAH_HD double ld(const S *p, long long i) {
     return (double)ldg(p + i);
@@ -69,7 +84,7 @@ VAH_HD double ld(const S *p, long long i) {
 template <typename S, bool IS3D>
 VAH_HD void load_cell_grad(const StageArgs<S> &a, long long s, CellGrad &g) {
     const long long sx = 1, sy = a.ncx, sz = a.plane;
-    const double fx = 1 / a.dx / 2, fy = 1 / a.dy / 2, fz = 1 / a.dz / 2;
+    const double fx = a.inv2h[0], fy = a.inv2h[1], fz = a.inv2h[2];
     const S *UT = a.uin[0], *UX = a.uin[1], *UY = a.uin[2], *UN = a.uin[3];
     g.e = ld(a.ein, s);
     g.p = ld(a.pin, s);
@@ -162,7 +177,7 @@ VAH_HD void stage_cell(const StageArgs<S> &a, int i, int j, int k) {
     // eulerStepKernelSource: q + dt S (FullyDiscreteKurganovTadmorScheme.cpp:43-122)
     CellGrad g;
     load_cell_grad<S, IS3D>(a, s, g);
-    int bad = cell_sources<PHYS>(a.eos, qc, g, a.t_src, a.dt, a.etabar, Sv);
+    int bad = cell_sources<PHYS>(a.eos, qc, g, a.ksrc, Sv);
 #pragma unroll
     for (int n = 0; n < NQ; ++n) val[n] = qc[n] + a.dt * Sv[n];
 
@@ -262,7 +277,7 @@ VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
     for (int n = 0; n < NQ; ++n) qc[n] = ld(a.qin[n], s);
     CellGrad g;
     load_cell_grad<S, IS3D>(a, s, g);
-    int bad = cell_sources<PHYS>(a.eos, qc, g, a.t_src, a.dt, a.etabar, Sv);
+    int bad = cell_sources<PHYS>(a.eos, qc, g, a.ksrc, Sv);
 #pragma unroll
     for (int n = 0; n < NQ; ++n) val[n] = qc[n] + a.dt * Sv[n];
     const long long strides[3] = {1, a.ncx, a.plane};
@@ -271,13 +286,13 @@ VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
 #pragma unroll
     for (int dir = 0; dir < (IS3D ? 3 : 2); ++dir) {
         const long long st = strides[dir];
-        const double c = a.dt / hs[dir];
+        const double c = a.c_h[dir];
         const S *const *Hm = EXACT ? a.HR[dir] : a.H[dir];  // face -1/2 as this cell evaluates it
 #pragma unroll
         for (int n = 0; n < NQ; ++n) val[n] += c * (ld(Hm[n], s - st) - ld(a.H[dir][n], s));
         if (Phys<PHYS>::PIMUNU) {
             double d[16];
-            const double f = 1 / hs[dir] / 2;
+            const double f = a.inv2h[dir];
 #pragma unroll
             for (int n = 5; n < NQ; ++n) d[n] = (ld(a.qin[n], s + st) - ld(a.qin[n], s - st)) * f;
             double Sa[4];

@@ -206,6 +206,7 @@ void hc_step(void *p, double t, double dt) {
     for (int n = 0; n < 16; ++n) { a.qin[n] = h->q[n]; a.qout[n] = h->qS[n]; }
     for (int m = 0; m < 4; ++m) { a.uin[m] = h->u[m]; a.upin[m] = h->up[m]; a.guess[m] = h->u[m]; a.uout[m] = h->uS[m]; }
     a.ein = h->ep[c][0]; a.pin = h->ep[c][1]; a.eout = h->ep[o][0]; a.pout = h->ep[o][1];
+    vah::finish_args(a);
     stage(h, a);
     common(h, a);
     set_regmap(h, a);
@@ -213,6 +214,7 @@ void hc_step(void *p, double t, double dt) {
     for (int n = 0; n < 16; ++n) { a.qin[n] = h->qS[n]; a.qavg[n] = h->q[n]; a.qout[n] = h->q[n]; }
     for (int m = 0; m < 4; ++m) { a.uin[m] = h->uS[m]; a.upin[m] = h->u[m]; a.guess[m] = h->u[m]; a.uout[m] = h->up[m]; }
     a.ein = h->ep[o][0]; a.pin = h->ep[o][1]; a.eout = h->ep[c][0]; a.pout = h->ep[c][1];
+    vah::finish_args(a);
     stage(h, a);
     if (h->validity) {
         vah::ValidityArgs<double> v;
