@@ -80,6 +80,19 @@ VAH_HD double ld(const S *p, long long i) {
     return (double)ldg(p + i);
 }
 
+// Face values are read once, by the cell launch: loaded with the streaming
+// (evict-first) cache policy, so that they do not push the state's neighbour
+// reuse out of L1 and L2 (cell launch 3% faster; streaming stores in the face
+// launches cost those 2%, so they store normally).
+template <typename S>
+VAH_HD double ld_stream(const S *p, long long i) {
+#ifdef __CUDA_ARCH__
+    return (double)__ldcs(p + i);
+#else
+    return (double)p[i];
+#endif
+}
+
 // Gradients and centre values the source terms need (SourceTerms.cpp:239-280, 484-486).
 template <typename S, bool IS3D>
 VAH_HD void load_cell_grad(const StageArgs<S> &a, long long s, CellGrad &g) {
@@ -289,7 +302,7 @@ VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
         const double c = a.c_h[dir];
         const S *const *Hm = EXACT ? a.HR[dir] : a.H[dir];  // face -1/2 as this cell evaluates it
 #pragma unroll
-        for (int n = 0; n < NQ; ++n) val[n] += c * (ld(Hm[n], s - st) - ld(a.H[dir][n], s));
+        for (int n = 0; n < NQ; ++n) val[n] += c * (ld_stream(Hm[n], s - st) - ld_stream(a.H[dir][n], s));
         if (Phys<PHYS>::PIMUNU) {
             double d[16];
             const double f = a.inv2h[dir];
