@@ -1,6 +1,6 @@
 """Event observables used to state the FP32 form's error against FP64.
 
-The reference defines none of these (SURVEY §7 hard part (v)); definitions:
+The reference defines none of these, so they are defined here:
 
     E_tot(tau)  = sum over interior cells of tau * T^{tau tau} dx dy deta
                   (the Milne energy; not conserved, it changes by
