@@ -239,4 +239,9 @@ void hc_counters(void *p, unsigned long long *out) {
     for (int k = 0; k < 3; ++k) out[k] = h->counters[k];
 }
 
+// The limiter of the device code over arrays of (x, y, z) triples.
+void hc_approx_derivative(const double *x, const double *y, const double *z, double *out, long long n) {
+    for (long long i = 0; i < n; ++i) out[i] = vah::approx_derivative(x[i], y[i], z[i]);
+}
+
 }  // extern "C"

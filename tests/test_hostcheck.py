@@ -87,3 +87,33 @@ def test_host_build_of_validity_code_matches_oracle(physics, eos, shape, split):
         h.step(0.5 + 0.02 * n, 0.02)
     errs = validity_errors(g, o.validity, h.validity)
     assert max(errs) < 1e-10, [(k, e) for k, e in enumerate(errs) if e >= 1e-10]
+
+
+def _minmod_reference(x, y):
+    """FluxLimiter.cpp:15-22: (sign x + sign y) min(|x|, |y|) / 2, sign(0) = +1."""
+    sx = np.where(x < 0, -1.0, 1.0)
+    sy = np.where(y < 0, -1.0, 1.0)
+    return (sx + sy) * np.minimum(np.abs(x), np.abs(y)) / 2
+
+
+def test_limiter_equals_the_nested_minmod():
+    """The device limiter (one sign test and a three-way min) against the
+    reference's minmod(1.1 (y - x), minmod((z - x)/2, 1.1 (z - y)))
+    (FluxLimiter.cpp:28-33) on edge values and a million random triples,
+    ties and tiny and huge scales included: equal values everywhere."""
+    edge = np.array([0.0, -0.0, 1.0, -1.0, 2.0, 3.0, 1e-300, -1e-300, 5e-324, -5e-324, 1e300, -1e300])
+    x, y, z = (a.ravel() for a in np.meshgrid(edge, edge, edge, indexing="ij"))
+    rng = np.random.default_rng(7)
+    n = 1_000_000
+    r = rng.uniform(-1, 1, (3, n))
+    kind = rng.integers(0, 6, n)
+    r[1] = np.where(kind == 1, r[0], r[1])          # y == x
+    r[2] = np.where(kind == 2, r[1], r[2])          # z == y
+    r[2] = np.where(kind == 3, r[0], r[2])          # z == x
+    r *= np.where(kind == 4, 1e-300, np.where(kind == 5, 1e300, 1.0))
+    x, y, z = (np.ascontiguousarray(np.concatenate([a, b])) for a, b in zip((x, y, z), r))
+    ref = _minmod_reference(1.1 * (y - x), _minmod_reference((z - x) * 0.5, 1.1 * (z - y)))
+    out = np.empty_like(x)
+    p = [a.ctypes.data_as(V.P) for a in (x, y, z, out)]
+    V.hostcheck_lib().hc_approx_derivative(*p, len(x))
+    assert np.array_equal(out, ref)

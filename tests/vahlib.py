@@ -231,6 +231,7 @@ def hostcheck_lib():
         L.hc_step.argtypes = [C.c_void_p, D, D]
         L.hc_counters.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
         L.hc_set_split.argtypes = [C.c_void_p, I]
+        L.hc_approx_derivative.argtypes = [P, P, P, P, C.c_longlong]
         _hc = L
     return _hc
 
