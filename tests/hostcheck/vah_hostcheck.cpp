@@ -239,6 +239,13 @@ void hc_counters(void *p, unsigned long long *out) {
     for (int k = 0; k < 3; ++k) out[k] = h->counters[k];
 }
 
+// The device regulator on one cell (shear + bulk): q[16] and u[4] in, q out;
+// with_maps selects the path that also reports the nine ratios.
+void hc_regulate(double t, double e, double p, double *q, const double *u, int with_maps) {
+    double maps[11];
+    vah::regulate<2>(t, e, p, q, u, with_maps ? maps : nullptr);
+}
+
 // The limiter of the device code over arrays of (x, y, z) triples.
 void hc_approx_derivative(const double *x, const double *y, const double *z, double *out, long long n) {
     for (long long i = 0; i < n; ++i) out[i] = vah::approx_derivative(x[i], y[i], z[i]);

@@ -117,3 +117,37 @@ def test_limiter_equals_the_nested_minmod():
     p = [a.ctypes.data_as(V.P) for a in (x, y, z, out)]
     V.hostcheck_lib().hc_approx_derivative(*p, len(x))
     assert np.array_equal(out, ref)
+
+
+def test_regulator_largest_ratio_path_equals_the_nine_divisions():
+    """The regulator's largest shear ratio taken as one division of the largest
+    numerator (the path without validity maps) gives the same regulated state,
+    bit for bit, as the nine divisions of the path that reports them: random
+    cells with shear from small to far above the regulation threshold, a
+    light-like pi.pi = 0 and an all-zero pi included."""
+    L = V.hostcheck_lib()
+    rng = np.random.default_rng(11)
+    cases = []
+    for k in range(20000):
+        e = 10 ** rng.uniform(-3, 3)
+        p = e / 3
+        q = np.zeros(16)
+        q[4] = p * rng.uniform(0.05, 1.5)
+        scale = e * 10 ** rng.uniform(-4, 1)
+        q[5:15] = scale * rng.standard_normal(10)
+        q[15] = scale * 0.1 * rng.standard_normal()
+        ux, uy, un = rng.normal(0, 1.0, 3) * [1, 1, 0.5]
+        t = rng.uniform(0.2, 5)
+        ut = np.sqrt(1 + ux * ux + uy * uy + t * t * un * un)
+        cases.append((t, e, p, q, np.array([ut, ux, uy, un])))
+    q0 = np.zeros(16)
+    q0[4] = 1.0
+    cases.append((1.0, 3.0, 1.0, q0, np.array([1.0, 0.0, 0.0, 0.0])))
+    ql = np.zeros(16)
+    ql[4], ql[5], ql[6], ql[7] = 1.0, 2.0, 1.0, 1.0  # pi.pi = 2^2 - 2 (1^2) - 2 (1^2) = 0 exactly
+    cases.append((1.0, 3.0, 1.0, ql, np.array([1.0, 0.0, 0.0, 0.0])))
+    for t, e, p, q, u in cases:
+        a, b = q.copy(), q.copy()
+        L.hc_regulate(t, e, p, a.ctypes.data_as(V.P), u.ctypes.data_as(V.P), 0)
+        L.hc_regulate(t, e, p, b.ctypes.data_as(V.P), u.ctypes.data_as(V.P), 1)
+        assert np.array_equal(a.view(np.int64), b.view(np.int64))

@@ -232,6 +232,7 @@ def hostcheck_lib():
         L.hc_counters.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
         L.hc_set_split.argtypes = [C.c_void_p, I]
         L.hc_approx_derivative.argtypes = [P, P, P, P, C.c_longlong]
+        L.hc_regulate.argtypes = [D, D, D, P, P, I]
         _hc = L
     return _hc
 
