@@ -59,6 +59,18 @@ def test_eos_table_argument_errors():
     assert L.vah_eos_table_build(4096, out.ctypes.data_as(V.P), out.size) == -1
 
 
+def test_math_check_argument_errors():
+    """vah_math_check rejects bad ranges and sizes before touching a device."""
+    import ctypes as C
+    L = V.library()
+    L.vah_math_check.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double)]
+    a, b = C.c_double(), C.c_double()
+    for lo, hi, n in [(0.0, 1.0, 16), (1.0, 1.0, 16), (2.0, 1.0, 16), (1.0, 2.0, 1), (-1.0, 2.0, 16)]:
+        assert L.vah_math_check(0, lo, hi, n, C.byref(a), C.byref(b)) == -1
+    assert L.vah_math_check(0, 1.0, 2.0, 16, None, C.byref(b)) == -1
+
+
 def test_initial_condition_generators():
     P = V.product
     e = P.optical_glauber(61, 61, 0.2, 0.2, b=7.0, e_peak=1190.0).reshape(61, 61)
