@@ -11,6 +11,11 @@ metric is interior cell-updates per second.
 Under torchrun each rank advances its own event (seed 1 + rank): events are
 independent, so multi-GPU is replicas with weak scaling and no data-path
 collective. Rank 0 prints one JSON line.
+
+--impl reference times the reference's own CPU step (oracle/_ref, compiled
+from the reference's sources) on the same event: one worker process per host
+core (bounded by memory), each advancing its own copy of the full grid, with
+the inputs built by the oracle library -- no product code is loaded.
 """
 import argparse
 import json
@@ -33,8 +38,8 @@ T0, DT, ETA_S = 0.25, 0.005, 0.16
 B_IMPACT = 7.0
 NQ = 16
 BYTES_PER_CELL_UPDATE = (5 * NQ + 32) * 8  # algorithmic HBM bytes, FP64 storage
-WORKLOAD = "vah 3+1D MC-Glauber Au+Au b=7fm 121x121x81 dx=0.1 deta=0.1 table-EoS shear+bulk FP64"
-SAMPLE_NZ = 5  # eta slices of the CPU sample slab
+WORKLOAD = ("vah 3+1D MC-Glauber Au+Au b=7fm 121x121x81 dx=0.1 deta=0.1 table-EoS shear+bulk FP64, "
+            "reference initialisation (P_L = 0.0154483 e, u = 0, pi = Pi = 0)")
 
 
 def parse():
@@ -164,21 +169,34 @@ def rank_seed(rank, base):
 
 
 # ------------------------------------------------------------ CPU baseline --
+def event_config(cells=NX * NY * NZ):
+    """The workload both arms time (identical dicts in both JSON lines)."""
+    return {"workload": WORKLOAD, "cells": cells, "tau0_fm": T0, "dt_fm": DT, "eta_over_s": ETA_S,
+            "b_fm": B_IMPACT, "seed": 1, "l2": "inputs larger than L2 (state 0.55 GB per event)"}
+
+
 def _ref_worker(args):
-    """Run the reference's own CPU step (oracle/_ref) on the sample slab."""
+    """One worker process: the reference's own CPU step (oracle/_ref, built from
+    the reference's sources; the C restatement where it was not built)
+    advancing its own copy of the full 121x121x81 event. The EoS table and the
+    initial condition come from the oracle library's copy of the workload's
+    generators (bit-identical to the library's), so this process maps no
+    product code."""
     conn, steps, warm, seed = args
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import vahlib as V
-    table = V.eos_table()
-    g = V.Grid(NX, NY, SAMPLE_NZ, DX, DX, DZ, ETA_S, physics="pimunu_pi", eos="table", zeta="crossover",
-               table=table)
+    table = V.oracle_eos_table()
+    g = V.Grid(NX, NY, NZ, DX, DX, DZ, ETA_S, physics="pimunu_pi", eos="table", zeta="crossover", table=table)
     use_ref = V.ref_available(g.physics, g.eos)
     impl = V.Reference(g) if use_ref else V.Oracle(g)
-    e = initial_energy_density(V.product, table, seed, NX, NY, SAMPLE_NZ).reshape(SAMPLE_NZ, NY, NX)
+    e_peak = V.table_energy_density(table, 0.6 / 0.197326938)
+    exy, _ = V.oracle_mc_glauber(NX, NY, DX, DX, B_IMPACT, seed, e_peak=e_peak, e_floor=0.0)
+    f = V.oracle_longitudinal(NZ, DZ)
+    e = (f[:, None] * exy[None, :]) + 1e-3
     full = np.zeros(g.shape)
-    full[2:-2, 2:-2, 2:-2] = e
-    p = np.interp(np.log(np.maximum(full, 1e-300)), table[1] + table[3] * np.arange(int(table[0])),
-                  table[8:8 + int(table[0])])
+    full[2:-2, 2:-2, 2:-2] = e.reshape(NZ, NY, NX)
+    n = int(table[0])
+    p = np.interp(np.log(np.maximum(full, 1e-300)), table[1] + table[3] * np.arange(n), table[8:8 + n])
     V.load_state(impl, {V.E: full.ravel(), V.PP: p.ravel(), V.UT: np.ones(g.ncell), V.PL: p.ravel()})
     if use_ref:
         impl.set_conserved(T0)  # the reference's own initialisation
@@ -197,13 +215,13 @@ def _ref_worker(args):
 
 
 def cpu_step_rate(workers, steps, warmup, seed=1):
-    """Spawned workers (one per host core used) step their own copy of the
-    sample slab in lockstep; returns (cell-updates/s, kind, per-step wall s)."""
+    """Spawned workers (one per host core used), each stepping its own copy of
+    the full event in lockstep; returns (cell-updates/s, kind, per-step wall s)."""
     ctx = mp.get_context("spawn")
     pipes, procs = [], []
     for w in range(workers):
         a, b = ctx.Pipe()
-        p = ctx.Process(target=_ref_worker, args=((b, steps, warmup, seed + w),))
+        p = ctx.Process(target=_ref_worker, args=((b, steps, warmup, seed),))
         p.start()
         pipes.append(a)
         procs.append(p)
@@ -219,8 +237,7 @@ def cpu_step_rate(workers, steps, warmup, seed=1):
             walls.append(time.perf_counter() - a)
     for p in procs:
         p.join(timeout=60)
-    cells = NX * NY * SAMPLE_NZ
-    rate = workers * cells * len(walls) / sum(walls)
+    rate = workers * NX * NY * NZ * len(walls) / sum(walls)
     return rate, kinds.pop(), walls
 
 
@@ -231,18 +248,49 @@ def host_cores():
         return os.cpu_count() or 1
 
 
+REF_WORKER_BYTES = 1.3e9  # resident size of one reference process on the full event (measured: 1.02 GB)
+
+
+def available_memory_bytes():
+    """MemAvailable, bounded by the cgroup limit when one is set."""
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+    except Exception:
+        pass
+    for path in ("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory/memory.limit_in_bytes"):
+        try:
+            with open(path) as f:
+                v = f.read().strip()
+            if v != "max":
+                lim = int(v)
+                if lim < (1 << 60):
+                    avail = lim if avail is None else min(avail, lim)
+        except Exception:
+            pass
+    return avail
+
+
 # -------------------------------------------------------------- main arms --
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    workers = max(1, min(host_cores(), 64))
+    cores = host_cores()
+    workers = max(1, min(cores, 64))
+    mem = available_memory_bytes()
+    if mem is not None:
+        workers = max(1, min(workers, int(0.6 * mem / REF_WORKER_BYTES)))
     rate, kind, walls = cpu_step_rate(workers, args.steps, args.warmup)
     ms = 1000 * statistics.mean(walls)
-    sample = f"{NX}x{NY}x{SAMPLE_NZ} central-eta slab of the workload per worker, one RK2 step per worker per step"
+    sample = (f"the full {NX}x{NY}x{NZ} event (seed 1) in each of {workers} worker processes, one RK2 step per worker "
+              f"per step, in lockstep; {cores} host cores")
     line = {"impl": "reference", "metric": "cell-updates/s", "value": rate, "unit": "cell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": NX * NY * NZ, "global_batch": 1, "parallelism": "replicas"},
+            "config": event_config(),
             "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": workers, "kind": kind,
                              "sample": sample},
             "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -501,7 +549,7 @@ def run_vah(args, rank, world, dist):
                    precision=prec,
                    flux={"per_cell": vah.VAH_FLUX_PER_CELL, "shared": vah.VAH_FLUX_SHARED,
                          "fused": vah.VAH_FLUX_PER_CELL_FUSED}[args.flux])
-    ev.init_from_e(T0, e0, vah.VAH_PL_ISOTROPIC)
+    ev.init_from_e(T0, e0, vah.VAH_PL_REFERENCE)  # as the reference initialises (the reference arm does the same)
     t = T0
     ev.run(t, DT, args.warmup)
     t += args.warmup * DT
@@ -561,10 +609,9 @@ def run_vah(args, rank, world, dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64-inversion" if prec == vah.VAH_FP32 else "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD if prec == vah.VAH_FP64 else WORKLOAD.replace("FP64", "FP32 state"),
-                       "cells": cells, "global_batch": world, "parallelism": "replicas",
-                       "l2": "inputs larger than L2 (state 0.55 GB per event)", "dt_fm": DT, "tau0_fm": T0,
-                       "faces": args.flux,
+            "config": event_config(cells) if prec == vah.VAH_FP64 else
+            dict(event_config(cells), workload=WORKLOAD.replace("FP64", "FP32 state")),
+            "launch": {"faces": args.flux, "global_batch": world, "parallelism": "replicas",
                        "autotune": {k: c for k, c in zip(("face_x", "face_y", "face_z", "cell"), tune)}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic_per_launch(cells, args.flux, args.precision),
@@ -584,9 +631,10 @@ def run_vah(args, rank, world, dist):
     if clk_summary:
         line["clocks"] = clk_summary
     if world == 1 and not args.no_cpu_baseline:
-        rate, kind, walls = cpu_step_rate(1, 2, 0)
+        rate, kind, walls = cpu_step_rate(1, 1, 0)
         line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": 1, "kind": kind,
-                                "sample": f"{NX}x{NY}x{SAMPLE_NZ} central-eta slab of the workload, 2 RK2 steps"}
+                                "sample": f"one RK2 step of the full {NX}x{NY}x{NZ} event on one core "
+                                          f"({walls[0]:.1f} s)"}
     print(json.dumps(line), flush=True)
 
 

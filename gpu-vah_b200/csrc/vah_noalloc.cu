@@ -16,9 +16,14 @@
 // host the name denotes a host-side stand-in), so the first call on each
 // device looks the address up with cudaGetSymbolAddress while that device is
 // current and caches it; that first call should therefore come before any
-// stream capture. All calls share the array and it keeps the last call's
+// stream capture. The cache is keyed on the device's context as well (its
+// driver-assigned unique id): after the caller resets the device
+// (cudaDeviceReset) the module may load at another address, and the next
+// call looks it up again -- so the first call after a reset should also come
+// before any capture. All calls share the array and it keeps the last call's
 // contents: the counters are cleared at the start of every call, and calls
 // whose work overlaps on the GPU (two streams, two host threads) race on it.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -37,16 +42,51 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[VAH_NOALLOC_SCR
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char *g_scratch_ptr[kMaxDevices] = {nullptr};
+unsigned long long g_scratch_ctx[kMaxDevices] = {0};  // context id the cached address belongs to
 
-// Device address of the scratch array on the current device (set-up on first use).
+// The two driver calls that identify the current context, resolved through
+// the runtime (the library does not link the driver library directly).
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// Unique id of the calling thread's current context (the device's primary
+// context after cudaSetDevice); called with g_setup_mutex held.
+int current_context_id(unsigned long long *id) {
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void **)&g_ctx_get_current, 12000,
+                                             cudaEnableDefault, &q1) != cudaSuccess ||
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", (void **)&g_ctx_get_id, 12000, cudaEnableDefault, &q2) !=
+                cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess) {
+            g_ctx_get_current = nullptr;
+            g_ctx_get_id = nullptr;
+            return VAH_ERR_CUDA;
+        }
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return VAH_ERR_CUDA;
+    if (g_ctx_get_id(ctx, id) != CUDA_SUCCESS) return VAH_ERR_CUDA;
+    return VAH_OK;
+}
+
+// Device address of the scratch array on the current device: looked up on
+// the first call in each context of the device (set-up), cached after.
 int scratch_address(int device, unsigned char **out) {
     if (device < 0 || device >= kMaxDevices) return VAH_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return VAH_ERR_CUDA;  // makes the primary context current
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[device]) {
+    unsigned long long ctx = 0;
+    int rc = current_context_id(&ctx);
+    if (rc != VAH_OK) return rc;
+    if (!g_scratch_ptr[device] || g_scratch_ctx[device] != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || p == nullptr) return VAH_ERR_CUDA;
         g_scratch_ptr[device] = (unsigned char *)p;
+        g_scratch_ctx[device] = ctx;
     }
     *out = g_scratch_ptr[device];
     return VAH_OK;
@@ -61,6 +101,7 @@ extern "C" int vah_stage_noalloc(const vah_lattice *lat, double eta_over_s, int 
                                  const vah_stage_buffers *buf, void *stream, long long *counts_out) {
     if (!lat || !buf || (stage != 1 && stage != 2) || !(dt > 0) || !(t > 0) || !(eta_over_s > 0)) return VAH_ERR_ARG;
     if (lat->nx < 1 || lat->ny < 1 || lat->nz < 1) return VAH_ERR_ARG;
+    if (!(lat->dx > 0) || !(lat->dy > 0) || !(lat->dz > 0)) return VAH_ERR_ARG;
     if (physics < VAH_IDEAL || physics > VAH_PIMUNU_PI) return VAH_ERR_ARG;
     if (eos != VAH_EOS_CONFORMAL && eos != VAH_EOS_TABLE) return VAH_ERR_ARG;
     if (eos == VAH_EOS_TABLE && !d_eos_table) return VAH_ERR_ARG;

@@ -270,11 +270,15 @@ VAH_HD void invert_setup(double t, const double *q, InvSetup &s) {
 // vah_math_check), times f -- three dependent operations instead of an IEEE
 // division. The correction only needs
 // to be accurate relative to itself: where the iteration stops it is ~1e-7 of
-// u_T, so its error moves the root by ~1e-21 relative. An fp that flushes to
-// zero gives an infinite correction, which the iteration's exit test turns
-// into the reference's fallback, as the IEEE quotient's overflow does.
+// u_T, so its error moves the root by ~1e-21 relative. The estimate flushes
+// subnormal inputs and results (.ftz), so outside |fp| in [2^-1000, 2^1001)
+// -- an exponent test on the integer pipe, essentially never taken -- the
+// correction is the IEEE quotient, as in the reference (a NaN or infinite fp
+// lands there too).
 VAH_HD double newton_correction(double f, double fp) {
 #ifdef __CUDA_ARCH__
+    const unsigned biased = ((unsigned)__double2hiint(fp) >> 20) & 0x7ffu;
+    if (biased - 23u > 2000u) return f / fp;
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(fp));
     y = fma(y, fma(-fp, y, 1.0), y);

@@ -422,11 +422,15 @@ int vah_ic_longitudinal(int nz, double dz, double eta_flat, double sigma_eta, do
  * 87,381 ghosted cells for a 3+1D grid with shear + bulk (N_q = 16) and
  * 131,071 for a 2+1D one; larger grids return VAH_ERR_TOO_LARGE.
  * The first call on a device looks up the array's device address (do it
- * before any stream capture). Calls share the array: calls whose work
+ * before any stream capture); the address is cached per device and context,
+ * so the first call after a cudaDeviceReset looks it up again (and should
+ * also come before any capture). Calls share the array: calls whose work
  * overlaps on the GPU race on it. Stage 1 then stage 2 with the buffer roles
  * of vah_rk2_step make one time step. The conformal temperature is the
  * correctly rounded fourth root here (the host-libm correction table of the
- * event path needs device memory). counts_out (host, 3 entries: face
+ * event path needs device memory), so with the conformal EoS the stage
+ * departs from the reference at the rounding of the temperature (a few 1e-13
+ * relative after two steps on the tested grids). counts_out (host, 3 entries: face
  * fallbacks, cell fallbacks, NaN cells; may be NULL) makes the call wait for
  * the stage and returns VAH_ERR_NAN when a NaN reached e or u. */
 #define VAH_NOALLOC_SCRATCH_BYTES (64u << 20)
@@ -451,8 +455,11 @@ int vah_stage_noalloc(const vah_lattice *lat, double eta_over_s, int physics, in
  * step) and 1/sqrt (hardware estimate + two steps), against CUDA's
  * IEEE-rounded reciprocal and square root, on n log-spaced inputs in
  * [lo, hi] (alternating sign for the reciprocal). Writes the largest relative
- * errors. No counterpart in the reference, which divides and takes square
- * roots in IEEE arithmetic on the CPU. */
+ * errors (0 where both results are equal, infinities included). Outside
+ * |x| in [2^-1000, 2^1001) the Newton correction divides in IEEE arithmetic;
+ * 1/sqrt is checked on [2^-1000, 2^1000] only (its callers pass values >= 1).
+ * No counterpart in the reference, which divides and takes square roots in
+ * IEEE arithmetic on the CPU. */
 int vah_math_check(int device, double lo, double hi, int n, double *max_rel_rcp, double *max_rel_rsqrt);
 
 /* Library version string. */

@@ -18,6 +18,8 @@
 #ifndef VAH_ORACLE_H
 #define VAH_ORACLE_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -63,6 +65,17 @@ int vo_infer(const vo_config *cfg, double t, const double *q, double ePrev, doub
              double *out /* e, p, ut, ux, uy, un */);
 double vo_approx_derivative(double qm, double q, double qp);
 void vo_eos_eval(const vo_config *cfg, double e, double *out /* p, T, cs2 */);
+
+/* The benchmark workloads' inputs (vo_inputs.c): the tabulated crossover
+ * EoS (layout of include/vah.h: n, ln e_0, 1/d ln e, d ln e, e_0, ln e_{n-1},
+ * e_{n-1}, 0, then p[n], T[n], c_s^2[n]), a seeded MC-Glauber transverse
+ * profile (nx*ny, x fastest) and the longitudinal plateau + Gaussian f(eta).
+ * Return 0, or -1 on a bad argument. */
+int vo_eos_table_build(int n, double *out, size_t out_len);
+int vo_ic_mc_glauber(int nx, int ny, double dx, double dy, double b, double sigma_nn_fm2, int A, double ws_R,
+                     double ws_a, double width, unsigned long long seed, double e_peak, double e_floor, double *e_xy,
+                     int *npart_out);
+int vo_ic_longitudinal(int nz, double dz, double eta_flat, double sigma_eta, double *f_eta);
 
 #ifdef __cplusplus
 }

@@ -15,7 +15,10 @@ import vahlib as V
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("lo,hi", [(1e-300, 1e300), (1.0, 1e32)])
+# The last two ranges cross the edges of the reciprocal estimate's band,
+# [2^-1000, 2^1001): subnormal and near-overflow inputs, where the Newton
+# correction must take the IEEE quotient (equal results, infinities included).
+@pytest.mark.parametrize("lo,hi", [(1e-300, 1e300), (1.0, 1e32), (4e-324, 1e-295), (1e295, 1.7e308)])
 def test_gpu_fast_reciprocal_and_rsqrt_error_bounds(lo, hi):
     L = V.library()
     L.vah_math_check.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.POINTER(C.c_double),

@@ -159,3 +159,19 @@ def test_validity_diagnostics_match_the_reference_bit_for_bit(physics, eos, shap
         np.testing.assert_array_equal(a, b, err_msg=f"validity field {vid}")
         nonzero += bool(np.any(b != 0))
     assert nonzero >= (27 if physics == "pimunu_pi" else 24)
+
+
+def test_oracle_workload_inputs_equal_the_library_generators_bit_for_bit():
+    """The oracle's copy of the workloads' inputs (the benchmark's reference
+    arm builds its event from it, loading no product code) equals the
+    library's host generators exactly: EoS table, MC-Glauber profile and
+    longitudinal profile."""
+    tab_o, tab_p = V.oracle_eos_table(), V.eos_table()
+    assert np.array_equal(tab_o, tab_p)
+    for b, seed in ((7.0, 1), (11.5, 12345)):
+        eo, no = V.oracle_mc_glauber(121, 117, 0.1, 0.1, b, seed, e_peak=1234.5, e_floor=1e-3)
+        ep, np_ = V.product.mc_glauber(121, 117, 0.1, 0.1, b, seed, e_peak=1234.5, e_floor=1e-3)
+        assert no == np_ and np.array_equal(eo, ep)
+    assert np.array_equal(V.oracle_longitudinal(81, 0.1), V.product.longitudinal(81, 0.1))
+    T = 0.6 / 0.197326938
+    assert V.table_energy_density(tab_o, T) == V.product.table_energy_density(tab_p, T)

@@ -71,8 +71,42 @@ def oracle_lib():
         L.vo_set_validity.argtypes = [C.c_void_p, I]
         L.vo_validity_field.restype = P
         L.vo_validity_field.argtypes = [C.c_void_p, I]
+        L.vo_eos_table_build.argtypes = [I, P, C.c_size_t]
+        L.vo_ic_mc_glauber.argtypes = [I, I, D, D, D, D, I, D, D, D, C.c_ulonglong, D, D, P, C.POINTER(I)]
+        L.vo_ic_longitudinal.argtypes = [I, D, D, D, P]
         _oracle = L
     return _oracle
+
+
+# The workloads' inputs built by the oracle library (no product code): the
+# reference arm of the benchmark uses these.
+def oracle_eos_table(n=4096):
+    out = np.zeros(8 + 3 * n)
+    assert oracle_lib().vo_eos_table_build(n, out.ctypes.data_as(P), out.size) == 0
+    return out
+
+
+def oracle_mc_glauber(nx, ny, dx, dy, b, seed, sigma_nn_fm2=4.2, A=197, R=6.38, a=0.535, width=0.5, e_peak=1.0,
+                      e_floor=1e-3):
+    out = np.zeros(nx * ny)
+    npart = C.c_int()
+    assert oracle_lib().vo_ic_mc_glauber(nx, ny, dx, dy, b, sigma_nn_fm2, A, R, a, width, seed, e_peak, e_floor,
+                                         out.ctypes.data_as(P), C.byref(npart)) == 0
+    return out, npart.value
+
+
+def oracle_longitudinal(nz, dz, eta_flat=1.5, sigma_eta=1.3):
+    out = np.zeros(nz)
+    assert oracle_lib().vo_ic_longitudinal(nz, dz, eta_flat, sigma_eta, out.ctypes.data_as(P)) == 0
+    return out
+
+
+def table_energy_density(tab, T_fm):
+    """e(T) by inverting a table's T(e) (interpolation in ln e)."""
+    n = int(tab[0])
+    Ts = tab[8 + n:8 + 2 * n]
+    lne = tab[1] + tab[3] * np.arange(n)
+    return float(np.exp(np.interp(np.log(T_fm), np.log(Ts), lne)))
 
 
 class Grid:
