@@ -41,6 +41,7 @@ struct vah_event {
     uint32_t *d_exc;
     int nexc;
     unsigned long long *d_counters;  // face fallbacks, cell fallbacks, NaN cells
+    unsigned char *d_fb;             // optional: per ghosted cell, stage-1 then stage-2 inversion fallback flags
     long long steps;
     double last_t, last_dt;          // time and step of the latest vah_rk2_step (autotuning state)
     double *d_stage64;               // FP32 storage: one FP64 field of staging for the host-buffer step
@@ -106,6 +107,7 @@ void free_all(vah_event *ev) {
     cudaFree(ev->d_tab);
     cudaFree(ev->d_exc);
     cudaFree(ev->d_counters);
+    cudaFree(ev->d_fb);
     cudaFree(ev->d_stage64);
     for (int m = 0; m < VAH_NUM_VALIDITY; ++m) cudaFree(ev->vd[m]);
     for (int n = 0; n < 16; ++n) cudaFree(ev->vq[n]);
@@ -266,6 +268,7 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->steps = 0;
     ev->last_t = hydro->t0;
     ev->d_stage64 = nullptr;
+    ev->d_fb = nullptr;
     ev->s_in = nullptr;
     ev->s_out = nullptr;
     ev->validity = false;
@@ -492,6 +495,7 @@ void stage1_args(const vah_event *ev, double t, double dt, StageArgs<S> &a) {
     a.pin = (const S *)ev->ep[c][1];
     a.eout = (S *)ev->ep[o][0];
     a.pout = (S *)ev->ep[o][1];
+    a.fallback = ev->d_fb;
     finish_args(a);
 }
 
@@ -520,6 +524,7 @@ void stage2_args(const vah_event *ev, double t, double dt, StageArgs<S> &a) {
     a.pin = (const S *)ev->ep[o][1];
     a.eout = (S *)ev->ep[c][0];
     a.pout = (S *)ev->ep[c][1];
+    a.fallback = ev->d_fb ? ev->d_fb + ev->ncell : nullptr;
     finish_args(a);
 }
 
@@ -718,6 +723,37 @@ extern "C" int vah_event_stats(vah_event *ev, vah_stats *out) {
     out->cell_fallbacks = (long long)c[1];
     out->nan_cells = (long long)c[2];
     out->steps = ev->steps;
+    return VAH_OK;
+}
+
+extern "C" int vah_event_track_fallbacks(vah_event *ev, int on) {
+    if (!ev) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(ev->opt.device));
+    if (on && !ev->d_fb) {
+        VAH_TRY(cudaMalloc((void **)&ev->d_fb, 2 * ev->ncell));
+        VAH_TRY(cudaMemsetAsync(ev->d_fb, 0, 2 * ev->ncell, ev->stream));
+    } else if (!on && ev->d_fb) {
+        VAH_TRY(cudaStreamSynchronize(ev->stream));
+        VAH_TRY(cudaFree(ev->d_fb));
+        ev->d_fb = nullptr;
+    }
+    return VAH_OK;
+}
+
+extern "C" int vah_event_get_fallback_mask(vah_event *ev, int stage, unsigned char *host, int with_ghosts) {
+    if (!ev || !host || (stage != 1 && stage != 2) || !ev->d_fb) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(ev->opt.device));
+    VAH_TRY(cudaStreamSynchronize(ev->stream));
+    const unsigned char *src = ev->d_fb + (stage - 1) * ev->ncell;
+    if (with_ghosts) {
+        VAH_TRY(cudaMemcpy(host, src, ev->ncell, cudaMemcpyDeviceToHost));
+        return VAH_OK;
+    }
+    const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz;
+    for (int k = 0; k < nz; ++k) {
+        const unsigned char *row = src + 2 + (size_t)ev->ncx * (2 + (size_t)ev->ncy * (k + 2));
+        VAH_TRY(cudaMemcpy2D(host + (size_t)nx * ny * k, nx, row, ev->ncx, nx, ny, cudaMemcpyDeviceToHost));
+    }
     return VAH_OK;
 }
 

@@ -137,7 +137,9 @@ __global__ void __launch_bounds__(kTX *kTY, MINB) batch_kernel(const SlotDesc<S>
                 const int gi = i + (KIND == K_FX ? 1 : 2), gj = j + (KIND == K_FY ? 1 : 2), gk = k + (KIND == K_FZ ? 1 : 2);
                 const long long st = KIND == K_FX ? 1 : (KIND == K_FY ? (long long)sa.ncx : sa.plane);
                 const long long s = gi + (long long)sa.ncx * gj + sa.plane * gk;
-                const unsigned fails = face_compute<S, PHYS, EXACT>(sa, s, KIND, st);
+                const int gl = KIND == K_FX ? gi : (KIND == K_FY ? gj : gk);
+                const int n = KIND == K_FX ? sa.nx : (KIND == K_FY ? sa.ny : sa.nz);
+                const unsigned fails = face_compute<S, PHYS, EXACT>(sa, s, KIND, st, gl >= 2, gl <= n);
                 if (fails & 255u) count_add(sa.counters + 0, fails & 255u);
                 if (fails >> 8) count_add(sa.counters + 2, 1ull);
             }

@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) face_kernel(const StageAr
     const int gi = i + (DIR == 0 ? 1 : 2), gj = j + (DIR == 1 ? 1 : 2), gk = k + (DIR == 2 ? 1 : 2);
     const long long st = DIR == 0 ? 1 : (DIR == 1 ? (long long)a.ncx : a.plane);
     const long long s = gi + (long long)a.ncx * gj + a.plane * gk;
-    const unsigned fails = face_compute<S, PHYS, EXACT>(a, s, DIR, st);
+    const int gl = DIR == 0 ? gi : (DIR == 1 ? gj : gk), n = DIR == 0 ? a.nx : (DIR == 1 ? a.ny : a.nz);
+    const unsigned fails = face_compute<S, PHYS, EXACT>(a, s, DIR, st, gl >= 2, gl <= n);
     if (a.counters) {
         if (fails & 255u) count_add(a.counters + 0, fails & 255u);
         if (fails >> 8) count_add(a.counters + 2, 1ull);

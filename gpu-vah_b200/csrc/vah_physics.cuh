@@ -55,6 +55,17 @@ VAH_HD double rsqrt_d(double x) {
 #endif
 }
 
+// 1/sqrt in the arithmetic type of the caller: rsqrt_d for FP64; in FP32 the
+// hardware's single-precision 1/sqrt (about 2 ulp) on the device.
+VAH_HD double rsqrt_r(double x) { return rsqrt_d(x); }
+VAH_HD float rsqrt_r(float x) {
+#ifdef __CUDA_ARCH__
+    return rsqrtf(x);
+#else
+    return 1.0f / sqrtf(x);
+#endif
+}
+
 VAH_HD uint32_t float_bits(float x) {
 #ifdef __CUDA_ARCH__
     return __float_as_uint(x);
@@ -110,51 +121,54 @@ VAH_HD double conformal_T(const Eos &eos, double e) {
     return (double)r;
 }
 
+template <typename R>
 struct EosPoint {
-    double p, T, cs2;
+    R p, T, cs2;
 };
 
 // Tabulated EoS: linear interpolation in ln e between nodes; power-law
 // continuation outside (p/e and c_s^2 frozen, T ~ e^(3/23) below, e^(1/4) above).
-template <bool NEED_P, bool NEED_TC>
-VAH_HD EosPoint table_lookup(const double *tab, double e) {
-    EosPoint r{0.0, 0.0, 0.0};
+// The table is FP64; R is the arithmetic type of the interpolation.
+template <bool NEED_P, bool NEED_TC, typename R>
+VAH_HD EosPoint<R> table_lookup(const double *tab, R e) {
+    EosPoint<R> r{R(0.0), R(0.0), R(0.0)};
     const int n = (int)ldg(tab);
     const double *P = tab + 8, *T = P + n, *C = T + n;
-    if (!(e > 0.0)) {
-        if (NEED_P) r.p = e * (ldg(P) / ldg(tab + 4));
-        if (NEED_TC) r.cs2 = ldg(C);
+    auto tl = [](const double *q) { return R(ldg(q)); };
+    if (!(e > R(0.0))) {
+        if (NEED_P) r.p = e * (tl(P) / tl(tab + 4));
+        if (NEED_TC) r.cs2 = tl(C);
         return r;
     }
-    const double x = log(e);
-    const double f = (x - ldg(tab + 1)) * ldg(tab + 2);
-    if (f <= 0.0) {
-        if (NEED_P) r.p = e * (ldg(P) / ldg(tab + 4));
+    const R x = log(e);
+    const R f = (x - tl(tab + 1)) * tl(tab + 2);
+    if (f <= R(0.0)) {
+        if (NEED_P) r.p = e * (tl(P) / tl(tab + 4));
         if (NEED_TC) {
-            r.T = ldg(T) * exp((3.0 / 23.0) * (x - ldg(tab + 1)));
-            r.cs2 = ldg(C);
+            r.T = tl(T) * exp((R(3.0) / R(23.0)) * (x - tl(tab + 1)));
+            r.cs2 = tl(C);
         }
         return r;
     }
-    if (f >= (double)(n - 1)) {
-        if (NEED_P) r.p = e * (ldg(P + n - 1) / ldg(tab + 6));
+    if (f >= (R)(n - 1)) {
+        if (NEED_P) r.p = e * (tl(P + n - 1) / tl(tab + 6));
         if (NEED_TC) {
-            r.T = ldg(T + n - 1) * exp(0.25 * (x - ldg(tab + 5)));
-            r.cs2 = ldg(C + n - 1);
+            r.T = tl(T + n - 1) * exp(R(0.25) * (x - tl(tab + 5)));
+            r.cs2 = tl(C + n - 1);
         }
         return r;
     }
     const int i = (int)f;
-    const double w = f - (double)i;
+    const R w = f - (R)i;
     if (NEED_P) {
-        double a = ldg(P + i), b = ldg(P + i + 1);
+        R a = tl(P + i), b = tl(P + i + 1);
         r.p = a + w * (b - a);
     }
     if (NEED_TC) {
-        double a = ldg(T + i), b = ldg(T + i + 1);
+        R a = tl(T + i), b = tl(T + i + 1);
         r.T = a + w * (b - a);
-        a = ldg(C + i);
-        b = ldg(C + i + 1);
+        a = tl(C + i);
+        b = tl(C + i + 1);
         r.cs2 = a + w * (b - a);
     }
     return r;
@@ -167,29 +181,31 @@ VAH_HD double eos_pressure(const Eos &eos, double e) {
 
 // (T, c_s^2); the conformal c_s^2 is the reference's integer `1/3` = 0
 // (EquationOfState.cpp:113).
-VAH_HD void eos_T_cs2(const Eos &eos, double e, double *T, double *cs2) {
+template <typename R>
+VAH_HD void eos_T_cs2(const Eos &eos, R e, R *T, R *cs2) {
     if (eos.kind == 0) {
-        *T = conformal_T(eos, e);
-        *cs2 = 0.0;
+        *T = R(conformal_T(eos, e));
+        *cs2 = R(0.0);
         return;
     }
-    EosPoint r = table_lookup<false, true>(eos.tab, e);
+    EosPoint<R> r = table_lookup<false, true>(eos.tab, e);
     *T = r.T;
     *cs2 = r.cs2;
 }
 
 // zeta/s(T), T in fm^-1: the reference's parameterisation (SourceTerms.cpp:
 // 22-44) or the crossover one (height 0.05 at 155 MeV, half-width 50 MeV).
-VAH_HD double zeta_over_s(const Eos &eos, double T) {
+template <typename R>
+VAH_HD R zeta_over_s(const Eos &eos, R T) {
     if (eos.zeta == 1) {
-        const double tp = 0.155 / kHbarc, w = 0.050 / kHbarc;
-        double d = (T - tp) / w;
-        return 0.05 / (1.0 + d * d);
+        const R tp = R(0.155) / R(kHbarc), w = R(0.050) / R(kHbarc);
+        R d = (T - tp) / w;
+        return R(0.05) / (R(1.0) + d * d);
     }
-    double x = T / 1.01355;
-    if (x > 1.05) return 0.9 * exp(-(x - 1) / 0.025) + 0.25 * exp(-(x - 1) / 0.13) + 0.001;
-    if (x < 0.995) return 0.9 * exp((x - 1) / 0.0025) + 0.22 * exp((x - 1) / 0.022) + 0.03;
-    return -13.77 * x * x + 27.55 * x - 13.45;
+    R x = T / R(1.01355);
+    if (x > R(1.05)) return R(0.9) * exp(-(x - 1) / R(0.025)) + R(0.25) * exp(-(x - 1) / R(0.13)) + R(0.001);
+    if (x < R(0.995)) return R(0.9) * exp((x - 1) / R(0.0025)) + R(0.22) * exp((x - 1) / R(0.022)) + R(0.03);
+    return -R(13.77) * x * x + R(27.55) * x - R(13.45);
 }
 
 // --------------------------------------------------------------- limiter --
@@ -205,12 +221,13 @@ VAH_HD double zeta_over_s(const Eos &eos, double T) {
 // With l = 1.1 (y - x) and r = 1.1 (z - y), min(|l|, |r|) is 1.1 min(|y - x|,
 // |z - y|) rounded once (rounding is monotone), and l, r have the signs of
 // y - x, z - y.
-VAH_HD double approx_derivative(double x, double y, double z) {
-    const double dl = y - x, dr = z - y;
-    const double c = (z - x) * 0.5;
-    const double m = fmin(1.1 * fmin(fabs(dl), fabs(dr)), fabs(c));
-    const bool neg = dl < 0.0;
-    return neg == (dr < 0.0) ? (neg ? -m : m) : 0.0;
+template <typename R>
+VAH_HD R approx_derivative(R x, R y, R z) {
+    const R dl = y - x, dr = z - y;
+    const R c = (z - x) * R(0.5);
+    const R m = fmin(R(1.1) * fmin(fabs(dl), fabs(dr)), fabs(c));
+    const bool neg = dl < R(0.0);
+    return neg == (dr < R(0.0)) ? (neg ? -m : m) : R(0.0);
 }
 
 // ------------------------------------------------------------- inversion --
@@ -468,10 +485,10 @@ VAH_HD int face_flux(double t, const double *qR, const double *qL, int dir, doub
 // ------------------------------------------------------- axis sources --
 // pi/Pi gradient terms of the T^{tau mu} equations along one axis
 // (SourceTerms.cpp:46-176). d[n] = (q[+1] - q[-1]) / (2h) for the pi fields.
-template <int PHYS>
-VAH_HD void axis_sources(const double *d, int dir, double ucomp, double ut, double t, double *S) {
-    const double v = ucomp / ut;
-    const double dPi = Phys<PHYS>::BULK ? d[kSlotPi] * 1.5 : 0.0;
+template <int PHYS, typename R>
+VAH_HD void axis_sources(const R *d, int dir, R ucomp, R ut, R t, R *S) {
+    const R v = ucomp / ut;
+    const R dPi = Phys<PHYS>::BULK ? d[kSlotPi] * R(1.5) : R(0.0);
     if (dir == 0) {
         S[0] = d[5] * v - d[6] - v * dPi;
         S[1] = d[6] * v - d[9] - dPi;
@@ -485,7 +502,7 @@ VAH_HD void axis_sources(const double *d, int dir, double ucomp, double ut, doub
     } else {
         const float tf = (float)t;  // SourceTerms.cpp:172: powf(t, 2)
         S[0] = d[5] * v - d[8] - v * dPi;
-        S[3] = d[8] * v - d[14] - dPi / (double)(tf * tf);
+        S[3] = d[8] * v - d[14] - dPi / (R)(tf * tf);
         S[1] = d[6] * v - d[11];
         S[2] = d[7] * v - d[13];
     }
@@ -494,200 +511,207 @@ VAH_HD void axis_sources(const double *d, int dir, double ucomp, double ut, doub
 // x / d for a constant d with its rounded reciprocal inv_d: the product and
 // one FMA correction (q + (x - q d) inv_d), within an ulp of the quotient
 // (usually the correctly rounded one), in three operations.
-VAH_HD double div_const(double x, double d, double inv_d) {
-    const double q = x * inv_d;
+template <typename R>
+VAH_HD R div_const(R x, R d, R inv_d) {
+    const R q = x * inv_d;
     return fma(fma(-q, d, x), inv_d, q);
 }
 
 // ----------------------------------------------------------- cell sources --
 // Inputs of the local source terms at one cell: stage-input conserved values,
 // primitives, previous-stage velocity and central differences (q(+1)-q(-1))/(2h).
-struct CellGrad {
-    double e, p, ut, ux, uy, un;
-    double utp, uxp, uyp, unp;
-    double dxut, dxux, dxuy, dxun, dyut, dyux, dyuy, dyun, dnut, dnux, dnuy, dnun;
-    double dxp, dyp, dnp, dxe, dye, dne, dxpl, dypl, dnpl;
+template <typename R>
+struct CellGradT {
+    R e, p, ut, ux, uy, un;
+    R utp, uxp, uyp, unp;
+    R dxut, dxux, dxuy, dxun, dyut, dyux, dyuy, dyun, dnut, dnux, dnuy, dnun;
+    R dxp, dyp, dnp, dxe, dye, dne, dxpl, dypl, dnpl;
 };
 
 // The sources' per-launch constants, formed once per launch with the same
 // operations as the per-cell expressions they stand for (bit-identical).
-struct StepConsts {
-    double t, dt, etabar, inv_t, inv_t2, inv_dt;
+template <typename R>
+struct StepConstsT {
+    R t, dt, etabar, inv_t, inv_t2, inv_dt;
 };
 
-VAH_HD StepConsts step_consts(double t, double dt, double etabar) {
-    StepConsts k;
+using CellGrad = CellGradT<double>;
+using StepConsts = StepConstsT<double>;
+
+template <typename R>
+VAH_HD StepConstsT<R> step_consts(R t, R dt, R etabar) {
+    StepConstsT<R> k;
     k.t = t;
     k.dt = dt;
     k.etabar = etabar;
-    k.inv_t = 1.0 / t;
-    k.inv_t2 = 1.0 / (t * t);
-    k.inv_dt = 1.0 / dt;
+    k.inv_t = R(1.0) / t;
+    k.inv_t2 = R(1.0) / (t * t);
+    k.inv_dt = R(1.0) / dt;
     return k;
 }
 
 // Geometric and relaxation sources S[n] (SourceTerms.cpp:178-1044), W off.
-template <int PHYS>
-VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, const StepConsts &k, double *S) {
-    const double t = k.t, etabar = k.etabar;
+template <int PHYS, typename R>
+VAH_HD int cell_sources(const Eos &eos, const R *Q, const CellGradT<R> &g, const StepConstsT<R> &k, R *S) {
+    const R t = k.t, etabar = k.etabar;
     constexpr bool PIM = Phys<PHYS>::PIMUNU, BULK = Phys<PHYS>::BULK;
-    const double ttt = Q[0], ttx = Q[1], tty = Q[2], ttn = Q[3], pl = Q[4];
-    double pitt = 0, pitx = 0, pity = 0, pitn = 0, pixx = 0, pixy = 0, pixn = 0, piyy = 0, piyn = 0, pinn = 0,
+    const R ttt = Q[0], ttx = Q[1], tty = Q[2], ttn = Q[3], pl = Q[4];
+    R pitt = 0, pitx = 0, pity = 0, pitn = 0, pixx = 0, pixy = 0, pixn = 0, piyy = 0, piyn = 0, pinn = 0,
            Pi = 0;
     if (PIM) {
         pitt = Q[5]; pitx = Q[6]; pity = Q[7]; pitn = Q[8]; pixx = Q[9];
         pixy = Q[10]; pixn = Q[11]; piyy = Q[12]; piyn = Q[13]; pinn = Q[14];
     }
     if (BULK) Pi = Q[kSlotPi];
-    double e = g.e;
-    const double p = g.p, ut = g.ut, ux = g.ux, uy = g.uy, un = g.un;
-    const double dxut = g.dxut, dxux = g.dxux, dxuy = g.dxuy, dxun = g.dxun;
-    const double dyut = g.dyut, dyux = g.dyux, dyuy = g.dyuy, dyun = g.dyun;
-    const double dnut = g.dnut, dnux = g.dnux, dnuy = g.dnuy, dnun = g.dnun;
+    R e = g.e;
+    const R p = g.p, ut = g.ut, ux = g.ux, uy = g.uy, un = g.un;
+    const R dxut = g.dxut, dxux = g.dxux, dxuy = g.dxuy, dxun = g.dxun;
+    const R dyut = g.dyut, dyux = g.dyux, dyuy = g.dyuy, dyun = g.dyun;
+    const R dnut = g.dnut, dnux = g.dnux, dnuy = g.dnuy, dnun = g.dnun;
 
-    const double inv_ut = 1.0 / ut, inv_t = k.inv_t;
-    const double vx = ux * inv_ut, vy = uy * inv_ut, vn = un * inv_ut;
-    const double dkvk = (dxux - vx * dxut) * inv_ut + (dyuy - vy * dyut) * inv_ut + (dnun - vn * dnut) * inv_ut;
+    const R inv_ut = R(1.0) / ut, inv_t = k.inv_t;
+    const R vx = ux * inv_ut, vy = uy * inv_ut, vn = un * inv_ut;
+    const R dkvk = (dxux - vx * dxut) * inv_ut + (dyuy - vy * dyut) * inv_ut + (dnun - vn * dnut) * inv_ut;
 
-    const double t2 = t * t, t3 = t * t2, un2 = un * un, ut2 = ut * ut;
-    const double inv_t2 = k.inv_t2;
+    const R t2 = t * t, t3 = t * t2, un2 = un * un, ut2 = ut * ut;
+    const R inv_t2 = k.inv_t2;
 
     // velocity gradients (SourceTerms.cpp:301-334)
-    const double inv_dt = k.inv_dt;
-    const double dtut = (ut - g.utp) * inv_dt, dtux = (ux - g.uxp) * inv_dt;
-    const double dtuy = (uy - g.uyp) * inv_dt, dtun = (un - g.unp) * inv_dt;
-    const double dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;
-    const double duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
-    const double dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
-    const double dut = ut * dtut + ux * dxut + uy * dyut + un * dnut;  // = Dut - t un^2
-    const double Dut = dut + t * un2;
-    const double Dux = -dux, Duy = -duy;
-    const double Dun = -t2 * (dun + 2 * ut * un * inv_t);
-    const double theta = ut * inv_t + dtut + dxux + dyuy + dnun;
-    const double th3 = div_const(theta, 3.0, 1.0 / 3.0);
+    const R inv_dt = k.inv_dt;
+    const R dtut = (ut - g.utp) * inv_dt, dtux = (ux - g.uxp) * inv_dt;
+    const R dtuy = (uy - g.uyp) * inv_dt, dtun = (un - g.unp) * inv_dt;
+    const R dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;
+    const R duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
+    const R dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
+    const R dut = ut * dtut + ux * dxut + uy * dyut + un * dnut;  // = Dut - t un^2
+    const R Dut = dut + t * un2;
+    const R Dux = -dux, Duy = -duy;
+    const R Dun = -t2 * (dun + 2 * ut * un * inv_t);
+    const R theta = ut * inv_t + dtut + dxux + dyuy + dnun;
+    const R th3 = div_const(theta, R(3.0), R(1.0) / R(3.0));
 
-    const double stt = -t * ut * un2 + (dtut - ut * dut) + (ut2 - 1) * th3;
-    const double stx = -(t * un2 * ux) * 0.5 + (dtux - dxut) * 0.5 - (ux * dut + ut * dux) * 0.5 + ut * ux * th3;
-    const double sty = -(t * un2 * uy) * 0.5 + (dtuy - dyut) * 0.5 - (uy * dut + ut * duy) * 0.5 + ut * uy * th3;
-    const double stn = -un * (2 * ut2 + t2 * un2) * (0.5 * inv_t) + (dtun - dnut * inv_t2) * 0.5 -
-                       (un * dut + ut * dun) * 0.5 + ut * un * th3;
-    const double sxx = -(dxux + ux * dux) + (1 + ux * ux) * th3;
-    const double sxy = -(dxuy + dyux) * 0.5 - (uy * dux + ux * duy) * 0.5 + ux * uy * th3;
-    const double sxn = -ut * ux * un * inv_t - (dxun + dnux * inv_t2) * 0.5 - (un * dux + ux * dun) * 0.5 + ux * un * th3;
-    const double syy = -(dyuy + uy * duy) + (1 + uy * uy) * th3;
-    const double syn = -ut * uy * un * inv_t - (dyun + dnuy * inv_t2) * 0.5 - (un * duy + uy * dun) * 0.5 + uy * un * th3;
-    const double snn = -ut * (1 + 2 * t2 * un2) / t3 - dnun * inv_t2 - un * dun + (inv_t2 + un2) * th3;
+    const R stt = -t * ut * un2 + (dtut - ut * dut) + (ut2 - 1) * th3;
+    const R stx = -(t * un2 * ux) * R(0.5) + (dtux - dxut) * R(0.5) - (ux * dut + ut * dux) * R(0.5) + ut * ux * th3;
+    const R sty = -(t * un2 * uy) * R(0.5) + (dtuy - dyut) * R(0.5) - (uy * dut + ut * duy) * R(0.5) + ut * uy * th3;
+    const R stn = -un * (2 * ut2 + t2 * un2) * (R(0.5) * inv_t) + (dtun - dnut * inv_t2) * R(0.5) -
+                       (un * dut + ut * dun) * R(0.5) + ut * un * th3;
+    const R sxx = -(dxux + ux * dux) + (1 + ux * ux) * th3;
+    const R sxy = -(dxuy + dyux) * R(0.5) - (uy * dux + ux * duy) * R(0.5) + ux * uy * th3;
+    const R sxn = -ut * ux * un * inv_t - (dxun + dnux * inv_t2) * R(0.5) - (un * dux + ux * dun) * R(0.5) + ux * un * th3;
+    const R syy = -(dyuy + uy * duy) + (1 + uy * uy) * th3;
+    const R syn = -ut * uy * un * inv_t - (dyun + dnuy * inv_t2) * R(0.5) - (un * duy + uy * dun) * R(0.5) + uy * un * th3;
+    const R snn = -ut * (1 + 2 * t2 * un2) / t3 - dnun * inv_t2 - un * dun + (inv_t2 + un2) * th3;
 
     // transverse / longitudinal split (SourceTerms.cpp:355-426)
-    const double uT2 = ux * ux + uy * uy;
-    const double uTdxuT = ux * dxux + uy * dxuy;
-    const double uTdyuT = ux * dyux + uy * dyuy;
-    const double uTdnuT = ux * dnux + uy * dnuy;
-    const double uTduT = ut * (ux * dtux + uy * dtuy) + ux * uTdxuT + uy * uTdyuT + un * uTdnuT;
-    const double F = 1 + uT2;
-    const double inv_F = 1.0 / F;
-    const double F2 = F * F;
-    const double inv_sF = rsqrt_d(F);
-    const double z0 = t * un * inv_sF;
-    const double z3 = ut * inv_t * inv_sF;
-    const double z02 = z0 * z0, z0z3 = z0 * z3, z32 = z3 * z3;
-    const double dz0 = (ut * un + t * dun - t * un * inv_F * uTduT) * inv_sF;
-    const double dz3 = (-ut2 * inv_t2 + dut * inv_t - ut * inv_t * inv_F * uTduT) * inv_sF;
-    const double Dz0 = dz0 + t * un * z3;
-    const double Dz3 = -t2 * (dz3 + (ut * z3 + un * z0) * inv_t);
-    const double A = z02 * stt - 2 * t2 * z0z3 * stn + t2 * t2 * z32 * snn;
-    const double B0 = z0 * stt - t2 * z3 * stn;
-    const double B1 = z0 * stx - t2 * z3 * sxn;
-    const double B2 = z0 * sty - t2 * z3 * syn;
-    const double B3 = z0 * stn - t2 * z3 * snn;
-    const double thetaT = 2 * th3 + A;
-    const double zDzu = theta - thetaT;
-    const double sttT = stt + 2 * z0 * B0 + z02 * A - 0.5 * (1 - ut * ut + z02) * A;
-    const double stxT = stx + z0 * B1 - 0.5 * (-ut * ux) * A;
-    const double styT = sty + z0 * B2 - 0.5 * (-ut * uy) * A;
-    const double stnT = stn + z0 * B3 + z3 * B0 + z0z3 * A - 0.5 * (-ut * un + z0z3) * A;
-    const double sxxT = sxx - 0.5 * (-1 - ux * ux) * A;
-    const double sxyT = sxy - 0.5 * (-ux * uy) * A;
-    const double sxnT = sxn + z3 * B1 - 0.5 * (-ux * un) * A;
-    const double syyT = syy - 0.5 * (-1 - uy * uy) * A;
-    const double synT = syn + z3 * B2 - 0.5 * (-uy * un) * A;
-    const double snnT = snn + 2 * z3 * B3 + z32 * A - 0.5 * (-inv_t2 - un * un + z32) * A;
+    const R uT2 = ux * ux + uy * uy;
+    const R uTdxuT = ux * dxux + uy * dxuy;
+    const R uTdyuT = ux * dyux + uy * dyuy;
+    const R uTdnuT = ux * dnux + uy * dnuy;
+    const R uTduT = ut * (ux * dtux + uy * dtuy) + ux * uTdxuT + uy * uTdyuT + un * uTdnuT;
+    const R F = 1 + uT2;
+    const R inv_F = R(1.0) / F;
+    const R F2 = F * F;
+    const R inv_sF = rsqrt_r(F);
+    const R z0 = t * un * inv_sF;
+    const R z3 = ut * inv_t * inv_sF;
+    const R z02 = z0 * z0, z0z3 = z0 * z3, z32 = z3 * z3;
+    const R dz0 = (ut * un + t * dun - t * un * inv_F * uTduT) * inv_sF;
+    const R dz3 = (-ut2 * inv_t2 + dut * inv_t - ut * inv_t * inv_F * uTduT) * inv_sF;
+    const R Dz0 = dz0 + t * un * z3;
+    const R Dz3 = -t2 * (dz3 + (ut * z3 + un * z0) * inv_t);
+    const R A = z02 * stt - 2 * t2 * z0z3 * stn + t2 * t2 * z32 * snn;
+    const R B0 = z0 * stt - t2 * z3 * stn;
+    const R B1 = z0 * stx - t2 * z3 * sxn;
+    const R B2 = z0 * sty - t2 * z3 * syn;
+    const R B3 = z0 * stn - t2 * z3 * snn;
+    const R thetaT = 2 * th3 + A;
+    const R zDzu = theta - thetaT;
+    const R sttT = stt + 2 * z0 * B0 + z02 * A - R(0.5) * (1 - ut * ut + z02) * A;
+    const R stxT = stx + z0 * B1 - R(0.5) * (-ut * ux) * A;
+    const R styT = sty + z0 * B2 - R(0.5) * (-ut * uy) * A;
+    const R stnT = stn + z0 * B3 + z3 * B0 + z0z3 * A - R(0.5) * (-ut * un + z0z3) * A;
+    const R sxxT = sxx - R(0.5) * (-1 - ux * ux) * A;
+    const R sxyT = sxy - R(0.5) * (-ux * uy) * A;
+    const R sxnT = sxn + z3 * B1 - R(0.5) * (-ux * un) * A;
+    const R syyT = syy - R(0.5) * (-1 - uy * uy) * A;
+    const R synT = syn + z3 * B2 - R(0.5) * (-uy * un) * A;
+    const R snnT = snn + 2 * z3 * B3 + z32 * A - R(0.5) * (-inv_t2 - un * un + z32) * A;
 
     // closures (SourceTerms.cpp:431-481)
-    if (e == 0) e = 1.e-7;
-    double T, cs2;
+    if (e == 0) e = R(1.e-7);
+    R T, cs2;
     eos_T_cs2(eos, e, &T, &cs2);
-    const double inv_e = 1.0 / e;
-    double ap[16];
-    ap[0] = 1.0;
+    const R inv_e = R(1.0) / e;
+    R ap[16];
+    ap[0] = R(1.0);
     ap[1] = pl * inv_e;
 #pragma unroll
     for (int k = 2; k < 16; ++k) ap[k] = ap[k - 1] * ap[1];
-    const double a = ap[1];
-    const double Rtilde = poly::Rtilde(ap);
-    const double Rbar0 = poly::Rbar0(ap);
-    const double Rgamma = poly::Rgamma(ap);
-    const double Rbar0P = poly::Rbar0P(ap);
+    const R a = ap[1];
+    const R Rtilde = poly::Rtilde(ap);
+    const R Rbar0 = poly::Rbar0(ap);
+    const R Rgamma = poly::Rgamma(ap);
+    const R Rbar0P = poly::Rbar0P(ap);
 
-    const double e3p = e - 3 * p;
-    const double ptHat = (e - pl - Rbar0 * e3p) * 0.5;
-    const double pt = ptHat + 1.5 * Pi;
-    const double DP = pl - pt;
-    const double Ltt = DP * t2 * un2 * inv_F;
-    const double Ltn = DP * ut * un * inv_F;
-    const double Lnn = DP * ut2 * inv_F * inv_t2;
-    const double tnn = (e + pt) * un * un + pt * inv_t2 + Lnn + pinn;
+    const R e3p = e - 3 * p;
+    const R ptHat = (e - pl - Rbar0 * e3p) * R(0.5);
+    const R pt = ptHat + R(1.5) * Pi;
+    const R DP = pl - pt;
+    const R Ltt = DP * t2 * un2 * inv_F;
+    const R Ltn = DP * ut * un * inv_F;
+    const R Lnn = DP * ut2 * inv_F * inv_t2;
+    const R tnn = (e + pt) * un * un + pt * inv_t2 + Lnn + pinn;
 
-    const double dxRbar0 = Rbar0P * (g.dxpl - a * g.dxe) * inv_e;
-    const double dyRbar0 = Rbar0P * (g.dypl - a * g.dye) * inv_e;
-    const double dnRbar0 = Rbar0P * (g.dnpl - a * g.dne) * inv_e;
-    const double dxptHat = 0.5 * (g.dxe - g.dxpl - Rbar0 * (g.dxe - 3 * g.dxp) - e3p * dxRbar0);
-    const double dyptHat = 0.5 * (g.dye - g.dypl - Rbar0 * (g.dye - 3 * g.dyp) - e3p * dyRbar0);
-    const double dnptHat = 0.5 * (g.dne - g.dnpl - Rbar0 * (g.dne - 3 * g.dnp) - e3p * dnRbar0);
-    const double dxDP = g.dxpl - dxptHat, dyDP = g.dypl - dyptHat, dnDP = g.dnpl - dnptHat;
+    const R dxRbar0 = Rbar0P * (g.dxpl - a * g.dxe) * inv_e;
+    const R dyRbar0 = Rbar0P * (g.dypl - a * g.dye) * inv_e;
+    const R dnRbar0 = Rbar0P * (g.dnpl - a * g.dne) * inv_e;
+    const R dxptHat = R(0.5) * (g.dxe - g.dxpl - Rbar0 * (g.dxe - 3 * g.dxp) - e3p * dxRbar0);
+    const R dyptHat = R(0.5) * (g.dye - g.dypl - Rbar0 * (g.dye - 3 * g.dyp) - e3p * dyRbar0);
+    const R dnptHat = R(0.5) * (g.dne - g.dnpl - Rbar0 * (g.dne - 3 * g.dnp) - e3p * dnRbar0);
+    const R dxDP = g.dxpl - dxptHat, dyDP = g.dypl - dyptHat, dnDP = g.dnpl - dnptHat;
 
-    const double inv_F2 = inv_F * inv_F;
-    const double dxLtt = (2 * DP * dxun * t2 * un) * inv_F + (dxDP * t2 * un2) * inv_F - (2 * DP * uTdxuT * t2 * un2) * inv_F2;
-    const double dyLtt = (2 * DP * dyun * t2 * un) * inv_F + (dyDP * t2 * un2) * inv_F - (2 * DP * uTdyuT * t2 * un2) * inv_F2;
-    const double dnLtt = (2 * DP * dnun * t2 * un) * inv_F + (dnDP * t2 * un2) * inv_F - (2 * DP * uTdnuT * t2 * un2) * inv_F2;
-    const double dxLtn = (DP * dxut * un) * inv_F + (DP * dxun * ut) * inv_F + (dxDP * un * ut) * inv_F -
+    const R inv_F2 = inv_F * inv_F;
+    const R dxLtt = (2 * DP * dxun * t2 * un) * inv_F + (dxDP * t2 * un2) * inv_F - (2 * DP * uTdxuT * t2 * un2) * inv_F2;
+    const R dyLtt = (2 * DP * dyun * t2 * un) * inv_F + (dyDP * t2 * un2) * inv_F - (2 * DP * uTdyuT * t2 * un2) * inv_F2;
+    const R dnLtt = (2 * DP * dnun * t2 * un) * inv_F + (dnDP * t2 * un2) * inv_F - (2 * DP * uTdnuT * t2 * un2) * inv_F2;
+    const R dxLtn = (DP * dxut * un) * inv_F + (DP * dxun * ut) * inv_F + (dxDP * un * ut) * inv_F -
                          (2 * DP * uTdxuT * un * ut) * inv_F2;
-    const double dyLtn = (DP * dyut * un) * inv_F + (DP * dyun * ut) * inv_F + (dyDP * un * ut) * inv_F -
+    const R dyLtn = (DP * dyut * un) * inv_F + (DP * dyun * ut) * inv_F + (dyDP * un * ut) * inv_F -
                          (2 * DP * uTdyuT * un * ut) * inv_F2;
-    const double dnLtn = (DP * dnut * un) * inv_F + (DP * dnun * ut) * inv_F + (dnDP * un * ut) * inv_F -
+    const R dnLtn = (DP * dnut * un) * inv_F + (DP * dnun * ut) * inv_F + (dnDP * un * ut) * inv_F -
                          (2 * DP * uTdnuT * un * ut) * inv_F2;
-    const double dnLnn = ((2 * DP * dnut * ut) * inv_F + (dnDP * ut2) * inv_F - (2 * DP * uTdnuT * ut2) * inv_F2) * inv_t2;
+    const R dnLnn = ((2 * DP * dnut * ut) * inv_F + (dnDP * ut2) * inv_F - (2 * DP * uTdnuT * ut2) * inv_F2) * inv_t2;
     (void)F2;
 
-    const double zeta_zz = Rtilde * e - 3 * pl;
-    const double zeta_zT = (Rtilde * e + pl) * 0.5;
-    const double delta_pipi = (3 + Rgamma) * 0.5;
-    const double tau_pipi = div_const(4 * delta_pipi, 3.0, 1.0 / 3.0);  // SourceTerms.cpp:634, 1/2 -> 0
-    const double lambda_pipi = Rgamma - 1;
-    const double taupiInv = 0.2 * T / etabar;
+    const R zeta_zz = Rtilde * e - 3 * pl;
+    const R zeta_zT = (Rtilde * e + pl) * R(0.5);
+    const R delta_pipi = (3 + Rgamma) * R(0.5);
+    const R tau_pipi = div_const(4 * delta_pipi, R(3.0), R(1.0) / R(3.0));  // SourceTerms.cpp:634, 1/2 -> 0
+    const R lambda_pipi = Rgamma - 1;
+    const R taupiInv = R(0.2) * T / etabar;
 
-    const double psT = pitt * sttT - 2 * pitx * stxT - 2 * pity * styT + pixx * sxxT + 2 * pixy * sxyT + piyy * syyT -
+    const R psT = pitt * sttT - 2 * pitx * stxT - 2 * pity * styT + pixx * sxxT + 2 * pixy * sxyT + piyy * syyT -
                        2 * pitn * stnT * t2 + 2 * pixn * sxnT * t2 + 2 * piyn * synT * t2 + pinn * snnT * t2 * t2;
 
-    double beta_lPi = 0, delta_lPi = 0, beta_PiPi = 0, delta_PiPi = 0, lambda_Pipi = 0;
+    R beta_lPi = 0, delta_lPi = 0, beta_PiPi = 0, delta_PiPi = 0, lambda_Pipi = 0;
     if (BULK) {
         // AnisotropicDistributionFunctions.cpp:73-190 (2/9 -> 0, 3/2 -> 1, 1/3 -> 0)
-        double third = 1.0 / 3.0 - cs2;
-        if (third == 0.0) third = 1.e-16;
-        const double meq2 = 36 * third;
-        const double z2logz = -2 * (1 + 0.02536 * meq2);
-        const double g40 = (poly::g0m2040DividedBym2LogZTerm(ap) * z2logz + poly::g0m2040DividedBym2Zm2Term(ap)) / meq2 +
+        R third = R(1.0) / R(3.0) - cs2;
+        if (third == R(0.0)) third = R(1.e-16);
+        const R meq2 = 36 * third;
+        const R z2logz = -2 * (1 + R(0.02536) * meq2);
+        const R g40 = (poly::g0m2040DividedBym2LogZTerm(ap) * z2logz + poly::g0m2040DividedBym2Zm2Term(ap)) / meq2 +
                            poly::g0m2040DividedBym2ConstantTerm(ap);
-        const double g20c = poly::g0m2020ConstantTerm(ap);
-        const double g20 = g20c + poly::g0m2020Z2LogZTerm(ap) * z2logz + poly::g0m2020Z2Term(ap) * meq2;
+        const R g20c = poly::g0m2020ConstantTerm(ap);
+        const R g20 = g20c + poly::g0m2020Z2LogZTerm(ap) * z2logz + poly::g0m2020Z2Term(ap) * meq2;
         beta_lPi = 3 * g40;
         delta_lPi = g20 + g40;
         beta_PiPi = 1 - g20c;
-        delta_PiPi = 0.5 * (1 + g20c);
-        lambda_Pipi = div_const(3 * poly::G_G1(ap), 5.0, 1.0 / 5.0) * (0 - cs2);
+        delta_PiPi = R(0.5) * (1 + g20c);
+        lambda_Pipi = div_const(3 * poly::G_G1(ap), R(5.0), R(1.0) / R(5.0)) * (0 - cs2);
     }
 
-    const double dPL = -(pl - p) * taupiInv + zeta_zz * zDzu - zeta_zT * thetaT - beta_lPi * Pi * zDzu -
+    const R dPL = -(pl - p) * taupiInv + zeta_zz * zDzu - zeta_zT * thetaT - beta_lPi * Pi * zDzu -
                        delta_lPi * Pi * thetaT - Rgamma * psT;
     S[4] = dPL * inv_ut + dkvk * pl;
 
@@ -701,56 +725,56 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, cons
 
     if (PIM) {
         // SourceTerms.cpp:725-930; the I6/I7 and lambda_piPi terms vanish with W off
-        const double etaBar_TC = ((3 - Rtilde) * e - 2 * pl) * 0.125;
-        const double I1tt = 2 * ut * (pitt * Dut + pitx * Dux + pity * Duy + pitn * Dun) - 2 * z0 * (pitt * Dz0 + pitn * Dz3);
-        const double I1tx = (pitt * ux + pitx * ut) * Dut + (pitx * ux + pixx * ut) * Dux + (pity * ux + pixy * ut) * Duy +
+        const R etaBar_TC = ((3 - Rtilde) * e - 2 * pl) * R(0.125);
+        const R I1tt = 2 * ut * (pitt * Dut + pitx * Dux + pity * Duy + pitn * Dun) - 2 * z0 * (pitt * Dz0 + pitn * Dz3);
+        const R I1tx = (pitt * ux + pitx * ut) * Dut + (pitx * ux + pixx * ut) * Dux + (pity * ux + pixy * ut) * Duy +
                             (pitn * ux + pixn * ut) * Dun - ((pitx * z0) * Dz0 + (pitn * ux + pixn * z0) * Dz3);
-        const double I1ty = (pitt * uy + pity * ut) * Dut + (pitx * uy + pixy * ut) * Dux + (pity * uy + piyy * ut) * Duy +
+        const R I1ty = (pitt * uy + pity * ut) * Dut + (pitx * uy + pixy * ut) * Dux + (pity * uy + piyy * ut) * Duy +
                             (pitn * uy + piyn * ut) * Dun - ((pity * z0) * Dz0 + (pitn * uy + piyn * z0) * Dz3);
-        const double I1tn = (pitt * un + pitn * ut) * Dut + (pitx * un + pixn * ut) * Dux + (pity * un + piyn * ut) * Duy +
+        const R I1tn = (pitt * un + pitn * ut) * Dut + (pitx * un + pixn * ut) * Dux + (pity * un + piyn * ut) * Duy +
                             (pitn * un + pinn * ut) * Dun - ((pitt * z3 + pitn * z0) * Dz0 + (pitn * z3 + pinn * z0) * Dz3);
-        const double I1xx = 2 * ux * (pitx * Dut + pixx * Dux + pixy * Duy + pixn * Dun);
-        const double I1xy = (pitx * uy + pity * ux) * Dut + (pixx * uy + pixy * ux) * Dux + (pixy * uy + piyy * ux) * Duy +
+        const R I1xx = 2 * ux * (pitx * Dut + pixx * Dux + pixy * Duy + pixn * Dun);
+        const R I1xy = (pitx * uy + pity * ux) * Dut + (pixx * uy + pixy * ux) * Dux + (pixy * uy + piyy * ux) * Duy +
                             (pixn * uy + piyn * ux) * Dun;
-        const double I1xn = (pitx * un + pitn * ux) * Dut + (pixx * un + pixn * ux) * Dux + (pixy * un + piyn * ux) * Duy +
+        const R I1xn = (pitx * un + pitn * ux) * Dut + (pixx * un + pixn * ux) * Dux + (pixy * un + piyn * ux) * Duy +
                             (pixn * un + pinn * ux) * Dun - ((pitx * z3) * Dz0 + (pixn * z3) * Dz3);
-        const double I1yy = 2 * uy * (pity * Dut + pixy * Dux + piyy * Duy + piyn * Dun);
-        const double I1yn = (pity * un + pitn * uy) * Dut + (pixy * un + pixn * uy) * Dux + (piyy * un + piyn * uy) * Duy +
+        const R I1yy = 2 * uy * (pity * Dut + pixy * Dux + piyy * Duy + piyn * Dun);
+        const R I1yn = (pity * un + pitn * uy) * Dut + (pixy * un + pixn * uy) * Dux + (piyy * un + piyn * uy) * Duy +
                             (piyn * un + pinn * uy) * Dun - ((pity * z3) * Dz0 + (piyn * z3) * Dz3);
-        const double I1nn = 2 * un * (pitn * Dut + pixn * Dux + piyn * Duy + pinn * Dun) - 2 * z3 * (pitn * Dz0 + pinn * Dz3);
+        const R I1nn = 2 * un * (pitn * Dut + pixn * Dux + piyn * Duy + pinn * Dun) - 2 * z3 * (pitn * Dz0 + pinn * Dz3);
 
-        const double ps2 = psT * 0.5;
-        const double I4tt = (pitt * sttT - pitx * stxT - pity * styT - t2 * pitn * stnT) - (1 - ut2 + z02) * ps2;
-        const double I4tx = (pitt * stxT + pitx * sttT) * 0.5 - (pitx * sxxT + pixx * stxT) * 0.5 -
-                            (pity * sxyT + pixy * styT) * 0.5 - t2 * (pitn * sxnT + pixn * stnT) * 0.5 + (ut * ux) * ps2;
-        const double I4ty = (pitt * styT + pity * sttT) * 0.5 - (pitx * sxyT + pixy * stxT) * 0.5 -
-                            (pity * syyT + piyy * styT) * 0.5 - t2 * (pitn * synT + piyn * stnT) * 0.5 + (ut * uy) * ps2;
-        const double I4tn = (pitt * stnT + pitn * sttT) * 0.5 - (pitx * sxnT + pixn * stxT) * 0.5 -
-                            (pity * synT + piyn * styT) * 0.5 - t2 * (pitn * snnT + pinn * stnT) * 0.5 +
+        const R ps2 = psT * R(0.5);
+        const R I4tt = (pitt * sttT - pitx * stxT - pity * styT - t2 * pitn * stnT) - (1 - ut2 + z02) * ps2;
+        const R I4tx = (pitt * stxT + pitx * sttT) * R(0.5) - (pitx * sxxT + pixx * stxT) * R(0.5) -
+                            (pity * sxyT + pixy * styT) * R(0.5) - t2 * (pitn * sxnT + pixn * stnT) * R(0.5) + (ut * ux) * ps2;
+        const R I4ty = (pitt * styT + pity * sttT) * R(0.5) - (pitx * sxyT + pixy * stxT) * R(0.5) -
+                            (pity * syyT + piyy * styT) * R(0.5) - t2 * (pitn * synT + piyn * stnT) * R(0.5) + (ut * uy) * ps2;
+        const R I4tn = (pitt * stnT + pitn * sttT) * R(0.5) - (pitx * sxnT + pixn * stxT) * R(0.5) -
+                            (pity * synT + piyn * styT) * R(0.5) - t2 * (pitn * snnT + pinn * stnT) * R(0.5) +
                             (ut * un - z0z3) * ps2;
-        const double I4xx = (pitx * stxT - pixx * sxxT - pixy * sxyT - t2 * pixn * sxnT) + (1 + ux * ux) * ps2;
-        const double I4xy = (pitx * styT + pity * stxT) * 0.5 - (pixx * sxyT + pixy * sxxT) * 0.5 -
-                            (pixy * syyT + piyy * sxyT) * 0.5 - t2 * (pixn * synT + piyn * sxnT) * 0.5 + (ux * uy) * ps2;
-        const double I4xn = (pitx * stnT + pitn * stxT) * 0.5 - (pixx * sxnT + pixn * sxxT) * 0.5 -
-                            (pixy * synT + piyn * sxyT) * 0.5 - t2 * (pixn * snnT + pinn * sxnT) * 0.5 + (ux * un) * ps2;
-        const double I4yy = (pity * styT - pixy * sxyT - piyy * syyT - t2 * piyn * synT) + (1 + uy * uy) * ps2;
-        const double I4yn = (pity * stnT + pitn * styT) * 0.5 - (pixy * sxnT + pixn * sxyT) * 0.5 -
-                            (piyy * synT + piyn * syyT) * 0.5 - t2 * (piyn * snnT + pinn * synT) * 0.5 + (uy * un) * ps2;
-        const double I4nn = (pitn * stnT - pixn * sxnT - piyn * synT - t2 * pinn * snnT) + (inv_t2 + un2 - z32) * ps2;
+        const R I4xx = (pitx * stxT - pixx * sxxT - pixy * sxyT - t2 * pixn * sxnT) + (1 + ux * ux) * ps2;
+        const R I4xy = (pitx * styT + pity * stxT) * R(0.5) - (pixx * sxyT + pixy * sxxT) * R(0.5) -
+                            (pixy * syyT + piyy * sxyT) * R(0.5) - t2 * (pixn * synT + piyn * sxnT) * R(0.5) + (ux * uy) * ps2;
+        const R I4xn = (pitx * stnT + pitn * stxT) * R(0.5) - (pixx * sxnT + pixn * sxxT) * R(0.5) -
+                            (pixy * synT + piyn * sxyT) * R(0.5) - t2 * (pixn * snnT + pinn * sxnT) * R(0.5) + (ux * un) * ps2;
+        const R I4yy = (pity * styT - pixy * sxyT - piyy * syyT - t2 * piyn * synT) + (1 + uy * uy) * ps2;
+        const R I4yn = (pity * stnT + pitn * styT) * R(0.5) - (pixy * sxnT + pixn * sxyT) * R(0.5) -
+                            (piyy * synT + piyn * syyT) * R(0.5) - t2 * (piyn * snnT + pinn * synT) * R(0.5) + (uy * un) * ps2;
+        const R I4nn = (pitn * stnT - pixn * sxnT - piyn * synT - t2 * pinn * snnT) + (inv_t2 + un2 - z32) * ps2;
 
-        const double c2 = delta_pipi * thetaT + lambda_pipi * zDzu;  // I2, I5 both scale pi
-        const double two_eta = 2 * etaBar_TC;
-        const double dpitt = two_eta * sttT - pitt * taupiInv - (I1tt - c2 * pitt + tau_pipi * I4tt) - 2 * un * t * pitn;
-        const double dpitx = two_eta * stxT - pitx * taupiInv - (I1tx - c2 * pitx + tau_pipi * I4tx) - un * t * pixn;
-        const double dpity = two_eta * styT - pity * taupiInv - (I1ty - c2 * pity + tau_pipi * I4ty) - un * t * piyn;
-        const double dpitn = two_eta * stnT - pitn * taupiInv - (I1tn - c2 * pitn + tau_pipi * I4tn) - un * t * pinn -
+        const R c2 = delta_pipi * thetaT + lambda_pipi * zDzu;  // I2, I5 both scale pi
+        const R two_eta = 2 * etaBar_TC;
+        const R dpitt = two_eta * sttT - pitt * taupiInv - (I1tt - c2 * pitt + tau_pipi * I4tt) - 2 * un * t * pitn;
+        const R dpitx = two_eta * stxT - pitx * taupiInv - (I1tx - c2 * pitx + tau_pipi * I4tx) - un * t * pixn;
+        const R dpity = two_eta * styT - pity * taupiInv - (I1ty - c2 * pity + tau_pipi * I4ty) - un * t * piyn;
+        const R dpitn = two_eta * stnT - pitn * taupiInv - (I1tn - c2 * pitn + tau_pipi * I4tn) - un * t * pinn -
                              (ut * pitn + un * pitt) * inv_t;
-        const double dpixx = two_eta * sxxT - pixx * taupiInv - (I1xx - c2 * pixx + tau_pipi * I4xx);
-        const double dpixy = two_eta * sxyT - pixy * taupiInv - (I1xy - c2 * pixy + tau_pipi * I4xy);
-        const double dpixn = two_eta * sxnT - pixn * taupiInv - (I1xn - c2 * pixn + tau_pipi * I4xn) - (ut * pixn + un * pitx) * inv_t;
-        const double dpiyy = two_eta * syyT - piyy * taupiInv - (I1yy - c2 * piyy + tau_pipi * I4yy);
-        const double dpiyn = two_eta * synT - piyn * taupiInv - (I1yn - c2 * piyn + tau_pipi * I4yn) - (ut * piyn + un * pity) * inv_t;
-        const double dpinn = two_eta * snnT - pinn * taupiInv - (I1nn - c2 * pinn + tau_pipi * I4nn) - 2 * (ut * pinn + un * pitn) * inv_t;
+        const R dpixx = two_eta * sxxT - pixx * taupiInv - (I1xx - c2 * pixx + tau_pipi * I4xx);
+        const R dpixy = two_eta * sxyT - pixy * taupiInv - (I1xy - c2 * pixy + tau_pipi * I4xy);
+        const R dpixn = two_eta * sxnT - pixn * taupiInv - (I1xn - c2 * pixn + tau_pipi * I4xn) - (ut * pixn + un * pitx) * inv_t;
+        const R dpiyy = two_eta * syyT - piyy * taupiInv - (I1yy - c2 * piyy + tau_pipi * I4yy);
+        const R dpiyn = two_eta * synT - piyn * taupiInv - (I1yn - c2 * piyn + tau_pipi * I4yn) - (ut * piyn + un * pity) * inv_t;
+        const R dpinn = two_eta * snnT - pinn * taupiInv - (I1nn - c2 * pinn + tau_pipi * I4nn) - 2 * (ut * pinn + un * pitn) * inv_t;
         S[5] = dpitt * inv_ut + pitt * dkvk;
         S[6] = dpitx * inv_ut + pitx * dkvk;
         S[7] = dpity * inv_ut + pity * dkvk;
@@ -764,12 +788,12 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, cons
     }
     if (BULK) {
         // SourceTerms.cpp:1030-1042
-        const double Rhat = poly::Rhat(ap);
-        const double bb = 1.0 / 3.0 - cs2;
-        const double tauPiInv = 15 * bb * bb * T / zeta_over_s(eos, T);
-        const double zeta_z = div_const((Rhat - Rbar0) * e3p, 3.0, 1.0 / 3.0);
-        const double zeta_T = div_const(-(Rbar0 + Rhat) * e3p, 6.0, 1.0 / 6.0);
-        const double dPi = -(div_const((1 - Rbar0) * e3p, 3.0, 1.0 / 3.0) + Pi) * tauPiInv - zeta_z * zDzu - zeta_T * thetaT -
+        const R Rhat = poly::Rhat(ap);
+        const R bb = R(1.0) / R(3.0) - cs2;
+        const R tauPiInv = 15 * bb * bb * T / zeta_over_s(eos, T);
+        const R zeta_z = div_const((Rhat - Rbar0) * e3p, R(3.0), R(1.0) / R(3.0));
+        const R zeta_T = div_const(-(Rbar0 + Rhat) * e3p, R(6.0), R(1.0) / R(6.0));
+        const R dPi = -(div_const((1 - Rbar0) * e3p, R(3.0), R(1.0) / R(3.0)) + Pi) * tauPiInv - zeta_z * zDzu - zeta_T * thetaT -
                            beta_PiPi * Pi * zDzu - delta_PiPi * Pi * thetaT + lambda_Pipi * psT;
         S[kSlotPi] = dPi * inv_ut + Pi * dkvk;
     }
@@ -782,35 +806,35 @@ VAH_HD int cell_sources(const Eos &eos, const double *Q, const CellGrad &g, cons
 // maps (optional, 11 values, written only with shear): the applied factor and
 // each criterion's own factor tanh(a)/a (1 below 1e-7) in the order
 // magnitude, trace, u-orthogonality x4, z-orthogonality x4 (:666-693).
-template <int PHYS>
-VAH_HD void regulate(double t, double &e, double &p, double *q, const double *u, double *maps = nullptr) {
-    if (e < 0.0) {
-        e = 1.e-7;
-        p = 1.e-7;
+template <int PHYS, typename R>
+VAH_HD void regulate(R t, R &e, R &p, R *q, const R *u, R *maps = nullptr) {
+    if (e < R(0.0)) {
+        e = R(1.e-7);
+        p = R(1.e-7);
     }
-    if (q[kSlotPL] < 0.0) q[kSlotPL] = 1.e-7;
+    if (q[kSlotPL] < R(0.0)) q[kSlotPL] = R(1.e-7);
     if (!Phys<PHYS>::PIMUNU) return;
-    const double pl = q[kSlotPL];
-    double ap[9];
-    ap[0] = 1.0;
+    const R pl = q[kSlotPL];
+    R ap[9];
+    ap[0] = R(1.0);
     ap[1] = pl / e;
 #pragma unroll
     for (int k = 2; k < 9; ++k) ap[k] = ap[k - 1] * ap[1];
-    const double ptHat = (e - pl - poly::Rbar0(ap) * (e - 3 * p)) * 0.5;
-    const double pitt = q[5], pitx = q[6], pity = q[7], pitn = q[8], pixx = q[9];
-    const double pixy = q[10], pixn = q[11], piyy = q[12], piyn = q[13], pinn = q[14];
-    const double ut = u[0], ux = u[1], uy = u[2], un = u[3];
-    const double inv_sF = rsqrt_d(1 + (ux * ux + uy * uy));
-    const double z0 = t * un * inv_sF;
-    const double z3 = ut / t * inv_sF;
-    const double t2 = t * t;
-    const double sTrsTrs = sqrt(fabs(e * e + pl * pl + 2 * ptHat * ptHat));
-    const double pipi = pitt * pitt - 2 * pitx * pitx - 2 * pity * pity + pixx * pixx + 2 * pixy * pixy + piyy * piyy -
+    const R ptHat = (e - pl - poly::Rbar0(ap) * (e - 3 * p)) * R(0.5);
+    const R pitt = q[5], pitx = q[6], pity = q[7], pitn = q[8], pixx = q[9];
+    const R pixy = q[10], pixn = q[11], piyy = q[12], piyn = q[13], pinn = q[14];
+    const R ut = u[0], ux = u[1], uy = u[2], un = u[3];
+    const R inv_sF = rsqrt_r(1 + (ux * ux + uy * uy));
+    const R z0 = t * un * inv_sF;
+    const R z3 = ut / t * inv_sF;
+    const R t2 = t * t;
+    const R sTrsTrs = sqrt(fabs(e * e + pl * pl + 2 * ptHat * ptHat));
+    const R pipi = pitt * pitt - 2 * pitx * pitx - 2 * pity * pity + pixx * pixx + 2 * pixy * pixy + piyy * piyy -
                         2 * pitn * pitn * t2 + 2 * pixn * pixn * t2 + 2 * piyn * piyn * t2 + pinn * pinn * t2 * t2;
-    const double spipi = sqrt(fabs(pipi));
-    double rho = spipi / sTrsTrs;
-    const double den = spipi;
-    const double num[9] = {pitt - pixx - piyy - pinn * t2,
+    const R spipi = sqrt(fabs(pipi));
+    R rho = spipi / sTrsTrs;
+    const R den = spipi;
+    const R num[9] = {pitt - pixx - piyy - pinn * t2,
                            -pitn * t2 * un + pitt * ut - pitx * ux - pity * uy,
                            -pixn * t2 * un + pitx * ut - pixx * ux - pixy * uy,
                            -piyn * t2 * un + pity * ut - pixy * ux - piyy * uy,
@@ -819,7 +843,7 @@ VAH_HD void regulate(double t, double &e, double &p, double *q, const double *u,
                            z0 * pitx - t2 * z3 * pixn,
                            z0 * pity - t2 * z3 * piyn,
                            z0 * pitn - t2 * z3 * pinn};
-    double cand[9];
+    R cand[9];
     if (maps) {  // every ratio is reported
 #pragma unroll
         for (int m = 0; m < 9; ++m) {
@@ -832,22 +856,22 @@ VAH_HD void regulate(double t, double &e, double &p, double *q, const double *u,
         // numerator divided once -- the same value bit for bit, NaN ratios
         // (0/0, NaN numerators) ignored as the comparisons ignore them, and
         // den = 0 giving +-inf as the nine quotients would.
-        double top = -INFINITY;
+        R top = -INFINITY;
 #pragma unroll
         for (int m = 0; m < 9; ++m)
             if (num[m] > top) top = num[m];
-        const double c = top / den;
+        const R c = top / den;
         if (c > rho) rho = c;
     }
-    double fac = tanh(rho) / rho;
-    if (rho < 1.e-7) fac = 1.0;
+    R fac = tanh(rho) / rho;
+    if (rho < R(1.e-7)) fac = R(1.0);
 #pragma unroll
     for (int n = 5; n < 15; ++n) q[n] *= fac;
     if (maps) {
-        const double a1 = spipi / sTrsTrs;
+        const R a1 = spipi / sTrsTrs;
         maps[0] = fac;
-        maps[1] = a1 < 1.e-7 ? 1.0 : tanh(a1) / a1;
-        for (int m = 0; m < 9; ++m) maps[2 + m] = cand[m] < 1.e-7 ? 1.0 : tanh(cand[m]) / cand[m];
+        maps[1] = a1 < R(1.e-7) ? R(1.0) : tanh(a1) / a1;
+        for (int m = 0; m < 9; ++m) maps[2 + m] = cand[m] < R(1.e-7) ? R(1.0) : tanh(cand[m]) / cand[m];
     }
 }
 

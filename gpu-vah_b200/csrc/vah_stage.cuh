@@ -252,9 +252,14 @@ VAH_HD void stage_cell(const StageArgs<S> &a, int i, int j, int k) {
 //     solver tolerance squared; where the reference's inversion falls back
 //     (dilute edges), shared faces do not reproduce it.
 
-// Face at +1/2 of ghosted cell s along axis dir (stride st).
+// Face at +1/2 of ghosted cell s along axis dir (stride st). left_in /
+// right_in: whether the cells on either side are interior cells. With
+// reference faces only interior cells' evaluations are needed (and counted,
+// as the reference counts them): the evaluation with a ghost cell's guess at
+// the first and last face of a row is skipped.
 template <typename S, int PHYS, bool EXACT>
-VAH_HD unsigned face_compute(const StageArgs<S> &a, long long s, int dir, long long st) {
+VAH_HD unsigned face_compute(const StageArgs<S> &a, long long s, int dir, long long st, bool left_in = true,
+                             bool right_in = true) {
     constexpr int NQ = Phys<PHYS>::NQ;
     double qR[NQ], qL[NQ], H[NQ];
 #pragma unroll
@@ -267,11 +272,14 @@ VAH_HD unsigned face_compute(const StageArgs<S> &a, long long s, int dir, long l
     InvSetup sR, sL;  // set up once, inverted from one guess (shared) or both (reference faces)
     invert_setup<PHYS>(a.t_src, qR, sR);
     invert_setup<PHYS>(a.t_src, qL, sL);
-    const double ux = ld(a.uin[1], s), uy = ld(a.uin[2], s);
-    unsigned fails = face_flux_setup<PHYS>(sR, sL, qR, qL, dir, ld(a.ein, s), sqrt(fabs(ux * ux + uy * uy)), H);
+    unsigned fails = 0;
+    if (!EXACT || left_in) {
+        const double ux = ld(a.uin[1], s), uy = ld(a.uin[2], s);
+        fails += face_flux_setup<PHYS>(sR, sL, qR, qL, dir, ld(a.ein, s), sqrt(fabs(ux * ux + uy * uy)), H);
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) a.H[dir][n][s] = (S)H[n];
-    if (EXACT) {
+        for (int n = 0; n < NQ; ++n) a.H[dir][n][s] = (S)H[n];
+    }
+    if (EXACT && right_in) {
         const double vx = ld(a.uin[1], s + st), vy = ld(a.uin[2], s + st);
         fails += face_flux_setup<PHYS>(sR, sL, qR, qL, dir, ld(a.ein, s + st), sqrt(fabs(vx * vx + vy * vy)), H);
 #pragma unroll

@@ -80,7 +80,8 @@ EXPORTS = ["vah_version", "vah_eos_table_build", "vah_event_create", "vah_event_
            "vah_event_kernel_time", "vah_rk2_step_host", "vah_ic_optical_glauber", "vah_ic_mc_glauber",
            "vah_ic_longitudinal", "vah_event_autotune", "vah_batch_autotune",
            "vah_batch_freezeout_volume", "vah_batch_fallback_mask", "vah_event_set_validity",
-           "vah_event_get_validity", "vah_batch_add_glauber", "vah_ic_mc_glauber_participants"]
+           "vah_event_get_validity", "vah_batch_add_glauber", "vah_ic_mc_glauber_participants",
+           "vah_event_track_fallbacks", "vah_event_get_fallback_mask"]
 
 _lib = None
 
@@ -112,6 +113,8 @@ def library():
         L.vah_run.argtypes = [C.c_void_p, D, D, I]
         L.vah_event_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.vah_event_set_timing.argtypes = [C.c_void_p, I]
+        L.vah_event_track_fallbacks.argtypes = [C.c_void_p, I]
+        L.vah_event_get_fallback_mask.argtypes = [C.c_void_p, I, C.POINTER(C.c_ubyte), I]
         L.vah_event_kernel_time.argtypes = [C.c_void_p, P, C.POINTER(C.c_longlong)]
         L.vah_rk2_step_host.argtypes = [C.c_void_p, D, D, C.POINTER(P)]
         L.vah_ic_optical_glauber.argtypes = [I, I, D, D, D, D, I, D, D, D, D, D, P]
@@ -225,6 +228,16 @@ class Event:
         s = Stats()
         check(self.L.vah_event_stats(self.ev, C.byref(s)), "vah_event_stats")
         return s
+
+    def track_fallbacks(self, on=True):
+        check(self.L.vah_event_track_fallbacks(self.ev, int(on)), "vah_event_track_fallbacks")
+
+    def fallback_mask(self, stage, with_ghosts=True):
+        """Per cell, 1 where the latest step's stage-`stage` inversion fell back (uint8)."""
+        out = np.empty(self.ncell if with_ghosts else self.nx * self.ny * self.nz, dtype=np.uint8)
+        check(self.L.vah_event_get_fallback_mask(self.ev, int(stage), out.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                                 int(with_ghosts)), "vah_event_get_fallback_mask")
+        return out
 
     def set_timing(self, on):
         check(self.L.vah_event_set_timing(self.ev, int(on)), "vah_event_set_timing")

@@ -121,9 +121,9 @@ typedef struct vah_options {
 } vah_options;
 
 typedef struct vah_stats {
-    long long face_fallbacks; /* face inversions that took the fallback, last step */
-    long long cell_fallbacks; /* cell inversions that took the fallback, last step */
-    long long nan_cells;      /* cells where a NaN reached e or u, last step */
+    long long face_fallbacks; /* face inversions that took the fallback, since the event was created */
+    long long cell_fallbacks; /* cell inversions that took the fallback, since the event was created */
+    long long nan_cells;      /* cells where a NaN reached e or u, since the event was created */
     long long steps;          /* steps taken since creation */
 } vah_stats;
 
@@ -183,6 +183,17 @@ int vah_run(vah_event *ev, double t0, double dt, int nsteps);
  * step produced a NaN. */
 int vah_event_sync(vah_event *ev);
 int vah_event_stats(vah_event *ev, vah_stats *out);
+
+/* Which cells took the inversion fallback: vah_event_track_fallbacks(ev, 1)
+ * allocates two bytes per ghosted cell and makes every following step record,
+ * per cell, whether the cell inversion of stage 1 and of stage 2 fell back to
+ * the reference's e = 0.999 e_prev, u = (1,0,0,0) (EnergyMomentumTensor.cpp:
+ * 163-172): the fTSolution flags setInferredVariablesKernel writes
+ * (EnergyMomentumTensor.cpp:199-268, :255-257); 0 frees them.
+ * vah_event_get_fallback_mask copies the flags of the latest step's stage
+ * (1 or 2) as bytes (1 = fell back), full ghosted array or interior only. */
+int vah_event_track_fallbacks(vah_event *ev, int on);
+int vah_event_get_fallback_mask(vah_event *ev, int stage, unsigned char *host, int with_ghosts);
 
 /* Device time (ms) of the stage kernels launched since the last call, and
  * how many launches; enabled by vah_event_set_timing(ev, 1). */
@@ -429,8 +440,8 @@ int vah_ic_longitudinal(int nz, double dz, double eta_flat, double sigma_eta, do
  * of vah_rk2_step make one time step. The conformal temperature is the
  * correctly rounded fourth root here (the host-libm correction table of the
  * event path needs device memory), so with the conformal EoS the stage
- * departs from the reference at the rounding of the temperature (a few 1e-13
- * relative after two steps on the tested grids). counts_out (host, 3 entries: face
+ * departs from the reference at the rounding of the temperature (a few
+ * 1e-10 relative on the shear stress after one step on the tested grid). counts_out (host, 3 entries: face
  * fallbacks, cell fallbacks, NaN cells; may be NULL) makes the call wait for
  * the stage and returns VAH_ERR_NAN when a NaN reached e or u. */
 #define VAH_NOALLOC_SCRATCH_BYTES (64u << 20)

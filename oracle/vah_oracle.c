@@ -34,6 +34,8 @@ struct vo_state {
     double *e, *p;
     double *u[4], *up[4], *uS[4];
     long long face_fail, cell_fail, nan_count;
+    long long face_fail_axis[3];  /* face_fail split by flux direction */
+    unsigned char *fallback[2];  /* per cell, 1 where stage 1 / stage 2's inversion fell back (last step) */
     int validity_on;
     double *vd[VO_NUM_VALIDITY];
 };
@@ -602,8 +604,10 @@ static void euler_step(vo_state *st, double t, double dt, double *const *cur, do
                     stencil_t sten;
                     double Hf[NQ_MAX], Hb[NQ_MAX], Hs[4], r[NQ_MAX];
                     gather(st, (const double *const *)cur, s, strides[dir], sten);
-                    st->face_fail += face_flux(st, t, sten, dir, 1, st->e[s], uT, Hf);
-                    st->face_fail += face_flux(st, t, sten, dir, 0, st->e[s], uT, Hb);
+                    const int ff = face_flux(st, t, sten, dir, 1, st->e[s], uT, Hf) +
+                                   face_flux(st, t, sten, dir, 0, st->e[s], uT, Hb);
+                    st->face_fail += ff;
+                    st->face_fail_axis[dir] += ff;
                     for (int n = 0; n < nq; ++n) {
                         r[n] = -Hf[n];
                         r[n] += Hb[n];
@@ -627,7 +631,8 @@ static void euler_step(vo_state *st, double t, double dt, double *const *cur, do
 
 /* EnergyMomentumTensor.cpp:199-268: invert every interior cell of q; the
  * Newton guess is |u_T| of `guess`, e (in place) is the fallback base. */
-static void infer_all(vo_state *st, double t, double *const *q, double *const *guess, double *const *out) {
+static void infer_all(vo_state *st, int stage, double t, double *const *q, double *const *guess,
+                      double *const *out) {
     for (int i = 2; i < st->ncx - 2; ++i)
         for (int j = 2; j < st->ncy - 2; ++j)
             for (int k = 2; k < st->ncz - 2; ++k) {
@@ -636,6 +641,7 @@ static void infer_all(vo_state *st, double t, double *const *q, double *const *g
                 for (int n = 0; n < st->nq; ++n) qs[n] = q[n][s];
                 double uT = sqrt(fabs(guess[1][s] * guess[1][s] + guess[2][s] * guess[2][s]));
                 int status = vo_infer(&st->cfg, t, qs, st->e[s], uT, v);
+                st->fallback[stage][s] = status != 0;
                 if (status != 0) st->cell_fail++;
                 if (status == 2) st->nan_count++;
                 st->e[s] = v[0];
@@ -899,9 +905,10 @@ static void ghosts(vo_state *st, double *const *q, double *const *u) {
  * (:791) write nothing the step reads and are not restated. */
 void vo_step(vo_state *st, double t, double dt) {
     st->face_fail = st->cell_fail = st->nan_count = 0;
+    st->face_fail_axis[0] = st->face_fail_axis[1] = st->face_fail_axis[2] = 0;
     euler_step(st, t, dt, st->q, st->qS, st->u, st->up);
     t += dt;
-    infer_all(st, t, st->qS, st->u, st->uS);
+    infer_all(st, 0, t, st->qS, st->u, st->uS);
     regulate(st, t, st->qS, st->uS);
     ghosts(st, st->qS, st->uS);
 
@@ -920,7 +927,7 @@ void vo_step(vo_state *st, double t, double dt) {
         st->up[m] = st->u[m];
         st->u[m] = tmp;
     }
-    infer_all(st, t, st->Q, st->up, st->u);
+    infer_all(st, 1, t, st->Q, st->up, st->u);
     regulate(st, t, st->Q, st->u);
     ghosts(st, st->Q, st->u);
     if (st->validity_on) check_validity(st, t, dt, st->q);  /* :791, before q and Q swap */
@@ -938,6 +945,14 @@ double vo_run(vo_state *st, double t0, double dt, int nsteps) {
     for (int n = 0; n < nsteps; ++n) vo_step(st, t0 + n * dt, dt);
     clock_gettime(CLOCK_MONOTONIC, &b);
     return (double)(b.tv_sec - a.tv_sec) + 1e-9 * (double)(b.tv_nsec - a.tv_nsec);
+}
+
+void vo_last_step_face_fallbacks(const vo_state *st, long long out[3]) {
+    for (int d = 0; d < 3; ++d) out[d] = st->face_fail_axis[d];
+}
+
+const unsigned char *vo_fallback_mask(const vo_state *st, int stage) {
+    return (stage == 1 || stage == 2) ? st->fallback[stage - 1] : NULL;
 }
 
 void vo_last_step_stats(const vo_state *st, long long out[3]) {
@@ -1004,6 +1019,8 @@ vo_state *vo_create(const vo_config *cfg) {
         st->up[m] = (double *)calloc(st->len, b);
         st->uS[m] = (double *)calloc(st->len, b);
     }
+    st->fallback[0] = (unsigned char *)calloc(st->len, 1);
+    st->fallback[1] = (unsigned char *)calloc(st->len, 1);
     return st;
 }
 
@@ -1013,6 +1030,8 @@ void vo_destroy(vo_state *st) {
     free(st->e); free(st->p);
     for (int m = 0; m < 4; ++m) { free(st->u[m]); free(st->up[m]); free(st->uS[m]); }
     for (int m = 0; m < VO_NUM_VALIDITY; ++m) free(st->vd[m]);
+    free(st->fallback[0]);
+    free(st->fallback[1]);
     free(st);
 }
 

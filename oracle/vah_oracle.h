@@ -51,6 +51,14 @@ double vo_run(vo_state *st, double t0, double dt, int nsteps);
 /* counts of inversion fallbacks / NaNs seen during the last step:
  * out[0] face (flux) fallbacks, out[1] cell fallbacks, out[2] NaNs */
 void vo_last_step_stats(const vo_state *st, long long out[3]);
+/* out[d]: the face fallbacks of the last step along axis d (x, y, eta). In
+ * 2+1D the reference still runs the eta sweep, whose fluxes are exact zeros,
+ * and its face inversions count here. */
+void vo_last_step_face_fallbacks(const vo_state *st, long long out[3]);
+/* per ghosted cell, 1 where the cell inversion of stage 1 or 2 of the last
+ * step took the reference's fallback (EnergyMomentumTensor.cpp:163-172),
+ * else 0; stage outside {1, 2}: NULL */
+const unsigned char *vo_fallback_mask(const vo_state *st, int stage);
 
 /* Validity diagnostics (HydrodynamicValidity.cpp:47-394, computed at the end
  * of every step, FullyDiscreteKurganovTadmorScheme.cpp:791) and the regulator

@@ -49,8 +49,9 @@ void run_stage_split(const vah::StageArgs<double> &a) {
         for (int k = (dir == 2 ? 1 : 2); k < a.nz + 2; ++k)
             for (int j = (dir == 1 ? 1 : 2); j < a.ny + 2; ++j)
                 for (int i = (dir == 0 ? 1 : 2); i < a.nx + 2; ++i) {
+                    const int gl = dir == 0 ? i : (dir == 1 ? j : k), n = dir == 0 ? a.nx : (dir == 1 ? a.ny : a.nz);
                     unsigned f = vah::face_compute<double, PHYS, EXACT>(a, i + (long long)a.ncx * j + a.plane * k,
-                                                                          dir, strides[dir]);
+                                                                          dir, strides[dir], gl >= 2, gl <= n);
                     a.counters[0] += f & 255u;
                 }
     for (int k = 0; k < a.nz; ++k)

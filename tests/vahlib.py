@@ -71,6 +71,9 @@ def oracle_lib():
         L.vo_set_validity.argtypes = [C.c_void_p, I]
         L.vo_validity_field.restype = P
         L.vo_validity_field.argtypes = [C.c_void_p, I]
+        L.vo_last_step_face_fallbacks.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+        L.vo_fallback_mask.restype = C.POINTER(C.c_ubyte)
+        L.vo_fallback_mask.argtypes = [C.c_void_p, I]
         L.vo_eos_table_build.argtypes = [I, P, C.c_size_t]
         L.vo_ic_mc_glauber.argtypes = [I, I, D, D, D, D, I, D, D, D, C.c_ulonglong, D, D, P, C.POINTER(I)]
         L.vo_ic_longitudinal.argtypes = [I, D, D, D, P]
@@ -170,6 +173,15 @@ class Oracle:
         out = (C.c_longlong * 3)()
         self.L.vo_last_step_stats(self.st, out)
         return list(out)
+
+    def face_fallbacks_by_axis(self):
+        out = (C.c_longlong * 3)()
+        self.L.vo_last_step_face_fallbacks(self.st, out)
+        return list(out)
+
+    def fallback_mask(self, stage):
+        """Per ghosted cell, 1 where the last step's stage-`stage` inversion fell back."""
+        return np.ctypeslib.as_array(self.L.vo_fallback_mask(self.st, stage), (self.g.ncell,)).copy()
 
     def set_validity(self, on):
         self.L.vo_set_validity(self.st, int(on))
