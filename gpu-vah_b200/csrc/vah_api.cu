@@ -3,6 +3,11 @@
 // An event owns its device state: conserved q (current) and qS (intermediate
 // stage), two (e, p) buffers used ping-pong across the two stages, and the
 // three velocity sets u (current), up (previous step) and uS (intermediate).
+// FP64 storage runs the face/cell split (or fused) kernels on the reference
+// layout. VAH_FP32 runs the FP32 form through the TMA-tiled stage kernel
+// (vah_tile.cuh): q and qS are then each one block of N_q fields, and every
+// field uses a row pitch padded to a multiple of 4 floats; the host-facing
+// copies convert to and from the reference layout.
 // No call ever exits or traps; failures come back as status codes.
 #include <cuda_runtime.h>
 
@@ -16,6 +21,7 @@
 #include "vah.h"
 #include "vah_kernels.cuh"
 #include "vah_powf_exc.h"
+#include "vah_tile.cuh"
 
 using vah::FieldSet;
 using vah::StageArgs;
@@ -56,6 +62,15 @@ struct vah_event {
     long long kernel_launches;
     cudaStream_t s_in, s_out;         // copy streams of the pipelined host-buffer step (created on first use)
     std::vector<cudaEvent_t> pev;     // its slab events
+    // FP32 form (tile layout)
+    bool tile;
+    void *qblock[2];                  // q and qS: nq fields each, ncell floats apart
+    vah::TileSlot h_tslot;            // the event's tile descriptor (host copy) ...
+    vah::TileSlot *d_tslot;           // ... and on the device
+    vah::TileItem *d_titems;
+    int ntitems;
+    unsigned *d_tcount, *d_terr;      // tile counter of a launch; kernel error flags
+    int tparity;                      // 0: u^n in the descriptor's uA; 1: in uB
 };
 
 namespace {
@@ -88,9 +103,17 @@ void *field_ptr(vah_event *ev, int id) {
 }
 
 void free_all(vah_event *ev) {
-    for (int n = 0; n < 16; ++n) {
-        cudaFree(ev->q[n]);
-        cudaFree(ev->qS[n]);
+    if (ev->tile) {
+        cudaFree(ev->qblock[0]);
+        cudaFree(ev->qblock[1]);
+        cudaFree(ev->d_tslot);
+        cudaFree(ev->d_titems);
+        cudaFree(ev->d_tcount);  // d_terr lives in the same allocation
+    } else {
+        for (int n = 0; n < 16; ++n) {
+            cudaFree(ev->q[n]);
+            cudaFree(ev->qS[n]);
+        }
     }
     for (int b = 0; b < 2; ++b)
         for (int m = 0; m < 2; ++m) cudaFree(ev->ep[b][m]);
@@ -154,8 +177,10 @@ void fill_common(const vah_event *ev, StageArgs<S> &a) {
         for (int m = 0; m < 11; ++m) a.regmap[m] = ev->vd[VAH_V_REGULATIONS + m];
 }
 
-template <typename S>
-int timed_launch(vah_event *ev, const StageArgs<S> &a) {
+// Run `launch` (the launches of one stage), bracketed by CUDA events on the
+// event's stream when timing is on.
+template <typename F>
+int timed(vah_event *ev, F launch) {
     cudaEvent_t *pair = nullptr;
     if (ev->timing) {
         if ((size_t)(ev->tev_used + 2) > ev->tev.size()) {
@@ -169,13 +194,81 @@ int timed_launch(vah_event *ev, const StageArgs<S> &a) {
         ev->tev_used += 2;
         VAH_TRY(cudaEventRecord(pair[0], ev->stream));
     }
-    if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED)
-        VAH_TRY(vah::launch_stage<S>(a, ev->opt.physics, ev->stream));
-    else
-        VAH_TRY(vah::launch_stage_split<S>(a, ev->opt.physics, ev->opt.flux == VAH_FLUX_PER_CELL, ev->split,
-                                           ev->stream));
+    VAH_TRY(launch());
     if (pair) VAH_TRY(cudaEventRecord(pair[1], ev->stream));
     return VAH_OK;
+}
+
+template <typename S>
+int timed_launch(vah_event *ev, const StageArgs<S> &a) {
+    return timed(ev, [&]() {
+        if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED) return vah::launch_stage<S>(a, ev->opt.physics, ev->stream);
+        return vah::launch_stage_split<S>(a, ev->opt.physics, ev->opt.flux == VAH_FLUX_PER_CELL, ev->split,
+                                          ev->stream);
+    });
+}
+
+// One stage of the FP32 form: the persistent tile launch over the event's tiles.
+int tile_stage(vah_event *ev, int stage, double t, double dt) {
+    const vah::TileClock clk0{t, ev->tparity, 1, ev->steps};
+    const vah::Eos eos = make_eos(ev);
+    return timed(ev, [&]() {
+        return vah::tile_launch(ev->d_tslot, nullptr, clk0, dt, ev->d_titems, ev->ntitems, ev->lat.nz > 1,
+                                ev->d_tcount, stage, ev->opt.physics, eos, ev->d_terr, ev->stream);
+    });
+}
+
+}  // namespace
+
+namespace {
+
+// Copy the host tile descriptor to the device (after a buffer role changes).
+int tile_sync_desc(vah_event *ev) {
+    VAH_TRY(cudaMemcpyAsync(ev->d_tslot, &ev->h_tslot, sizeof(vah::TileSlot), cudaMemcpyHostToDevice, ev->stream));
+    VAH_TRY(cudaStreamSynchronize(ev->stream));  // the host copy may change again
+    return VAH_OK;
+}
+
+// The tile descriptor, tensor maps and work-list of an FP32 event.
+int tile_setup(vah_event *ev) {
+    vah::TileSlot &d = ev->h_tslot;
+    memset(&d, 0, sizeof(d));
+    for (int b = 0; b < 2; ++b) {
+        d.Q[b] = (float *)ev->qblock[b];
+        const int rc = vah::tile_encode_q(&d.tmQ[b], d.Q[b], ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->ncx,
+                                          (long long)ev->ncell, ev->nq);
+        if (rc != VAH_OK) return rc;
+    }
+    for (int b = 0; b < 2; ++b)
+        for (int m = 0; m < 2; ++m) d.ep[b][m] = (float *)ev->ep[b == 0 ? ev->cur : 1 - ev->cur][m];
+    for (int m = 0; m < 4; ++m) {
+        d.uA[m] = (float *)ev->u[m];
+        d.uB[m] = (float *)ev->up[m];
+        d.uS[m] = (float *)ev->uS[m];
+    }
+    d.fstride = (long long)ev->ncell;
+    d.nx = ev->lat.nx;
+    d.ny = ev->lat.ny;
+    d.nz = ev->lat.nz;
+    d.pitch = ev->ncx;
+    d.ncy = ev->ncy;
+    d.nq = ev->nq;
+    d.dx = ev->lat.dx;
+    d.dy = ev->lat.dy;
+    d.dz = ev->lat.dz;
+    d.dt = 0.0;  // events pass their step with each launch
+    d.etabar = ev->hydro.eta_over_s;
+    d.counters = ev->d_counters;
+    VAH_TRY(cudaMalloc((void **)&ev->d_tslot, sizeof(vah::TileSlot)));
+    std::vector<vah::TileItem> items;
+    vah::tile_items(items, 0, ev->lat.nx, ev->lat.ny, ev->lat.nz);
+    ev->ntitems = (int)items.size();
+    VAH_TRY(cudaMalloc((void **)&ev->d_titems, items.size() * sizeof(vah::TileItem)));
+    VAH_TRY(cudaMemcpy(ev->d_titems, items.data(), items.size() * sizeof(vah::TileItem), cudaMemcpyHostToDevice));
+    VAH_TRY(cudaMalloc((void **)&ev->d_tcount, 2 * sizeof(unsigned)));
+    ev->d_terr = ev->d_tcount + 1;
+    VAH_TRY(cudaMemset(ev->d_tcount, 0, 2 * sizeof(unsigned)));
+    return tile_sync_desc(ev);
 }
 
 }  // namespace
@@ -231,6 +324,60 @@ extern "C" int vah_math_check(int device, double lo, double hi, int n, double *m
     return VAH_OK;
 }
 
+namespace {
+
+// FP64 FMA throughput: every thread runs 8 independent chains of `iters`
+// dependent FMAs (enough independent work to hide the FMA latency at full
+// occupancy); the result is folded into one store so the chains stay live.
+__global__ void __launch_bounds__(256) fp64_fma_kernel(double *out, int iters, double a, double b) {
+    double x[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x[c] = (threadIdx.x + blockIdx.x * 7 + c) * 1e-3;
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) x[c] = fma(x[c], a, b);
+    double s = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s += x[c];
+    if (s == 12345.678) out[0] = s;  // practically never: keeps the chains from being removed
+}
+
+}  // namespace
+
+extern "C" int vah_fp64_peak(int device, double *tflops, double *ms) {
+    if (!tflops || !ms) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(device));
+    int sms = 0;
+    VAH_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    double *d_out = nullptr;
+    VAH_TRY(cudaMalloc((void **)&d_out, sizeof(double)));
+    cudaEvent_t e0, e1;
+    int rc = VAH_OK;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = VAH_ERR_CUDA;
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    if (rc == VAH_OK) {
+        fp64_fma_kernel<<<blocks, threads>>>(d_out, iters / 16, 0.999999, 1e-7);  // warm-up
+        double best = 1e30;
+        for (int r = 0; r < 5 && rc == VAH_OK; ++r) {
+            float m = 0;
+            if (cudaEventRecord(e0) != cudaSuccess) rc = VAH_ERR_CUDA;
+            fp64_fma_kernel<<<blocks, threads>>>(d_out, iters, 0.999999, 1e-7);
+            if (cudaEventRecord(e1) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&m, e0, e1) != cudaSuccess)
+                rc = VAH_ERR_CUDA;
+            best = std::min(best, (double)m);
+        }
+        if (rc == VAH_OK) {
+            *ms = best;
+            *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3) / 1e12;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d_out);
+    return rc;
+}
+
 extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, const vah_options *opt,
                                 const double *eos_table, vah_event **out) {
     if (!lat || !hydro || !opt || !out) return VAH_ERR_ARG;
@@ -255,7 +402,8 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->hydro = *hydro;
     ev->opt = *opt;
     ev->nq = nq_of(opt->physics);
-    ev->ncx = lat->nx + 4;
+    ev->tile = opt->precision == VAH_FP32;
+    ev->ncx = ev->tile ? vah::tile_pitch(lat->nx) : lat->nx + 4;  // row pitch of the device arrays
     ev->ncy = lat->ny + 4;
     ev->ncz = lat->nz + 4;
     ev->ncell = (size_t)ev->ncx * ev->ncy * ev->ncz;
@@ -277,6 +425,12 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->last_dt = 0.005;
     ev->split = vah::default_split_config();
     ev->nexc = 0;
+    ev->qblock[0] = ev->qblock[1] = nullptr;
+    ev->d_tslot = nullptr;
+    ev->d_titems = nullptr;
+    ev->d_tcount = ev->d_terr = nullptr;
+    ev->ntitems = 0;
+    ev->tparity = 0;
     ev->own_stream = opt->stream == nullptr;
     int rc = VAH_OK;
     auto alloc = [&](void **p) {
@@ -290,11 +444,24 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     } else {
         ev->stream = (cudaStream_t)opt->stream;
     }
-    for (int n = 0; n < 16; ++n)
-        if (n < ev->nq || (n == VAH_F_PI && ev->nq == 16)) {
-            alloc(&ev->q[n]);
-            alloc(&ev->qS[n]);
+    if (ev->tile) {  // q and qS as blocks of nq fields (one tensor map each)
+        for (int b = 0; b < 2 && rc == VAH_OK; ++b) {
+            cudaError_t e = cudaMalloc(&ev->qblock[b], ev->nq * ev->ncell * sizeof(float));
+            if (e == cudaSuccess) e = cudaMemset(ev->qblock[b], 0, ev->nq * ev->ncell * sizeof(float));
+            if (e != cudaSuccess) rc = cuda_status(e);
         }
+        if (rc == VAH_OK)
+            for (int n = 0; n < ev->nq; ++n) {
+                ev->q[n] = (float *)ev->qblock[0] + n * ev->ncell;
+                ev->qS[n] = (float *)ev->qblock[1] + n * ev->ncell;
+            }
+    } else {
+        for (int n = 0; n < 16; ++n)
+            if (n < ev->nq || (n == VAH_F_PI && ev->nq == 16)) {
+                alloc(&ev->q[n]);
+                alloc(&ev->qS[n]);
+            }
+    }
     for (int b = 0; b < 2; ++b)
         for (int m = 0; m < 2; ++m) alloc(&ev->ep[b][m]);
     for (int m = 0; m < 4; ++m) {
@@ -302,7 +469,7 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
         alloc(&ev->up[m]);
         alloc(&ev->uS[m]);
     }
-    if (opt->flux != VAH_FLUX_PER_CELL_FUSED)
+    if (opt->flux != VAH_FLUX_PER_CELL_FUSED && !ev->tile)
         for (int d = 0; d < (lat->nz > 1 ? 3 : 2); ++d)
             for (int n = 0; n < ev->nq; ++n) {
                 alloc(&ev->H[d][n]);
@@ -327,6 +494,7 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
                 rc = VAH_ERR_CUDA;
         }
     }
+    if (rc == VAH_OK && ev->tile) rc = tile_setup(ev);
     if (rc != VAH_OK) {
         free_all(ev);
         delete ev;
@@ -351,7 +519,7 @@ namespace {
 // storage type; FP32 storage converts through a host staging buffer.
 int copy_field(vah_event *ev, void *d, double *host_out, const double *host_in, int with_ghosts) {
     const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz;
-    const size_t full = ev->ncell, inner = (size_t)nx * ny * nz;
+    const size_t full = (size_t)(nx + 4) * ev->ncy * ev->ncz, inner = (size_t)nx * ny * nz;  // host layouts
     const size_t n = with_ghosts ? full : inner;
     const bool to_dev = host_in != nullptr;
     std::vector<float> stage;
@@ -363,9 +531,12 @@ int copy_field(vah_event *ev, void *d, double *host_out, const double *host_in, 
     const void *src_h = ev->elem == sizeof(float) ? (const void *)stage.data() : (const void *)host_in;
     void *dst_h = ev->elem == sizeof(float) ? (void *)stage.data() : (void *)host_out;
     const size_t es = ev->elem;
-    if (with_ghosts) {
-        if (to_dev) VAH_TRY(cudaMemcpyAsync(d, src_h, full * es, cudaMemcpyHostToDevice, ev->stream));
-        else VAH_TRY(cudaMemcpyAsync(dst_h, d, full * es, cudaMemcpyDeviceToHost, ev->stream));
+    if (with_ghosts) {  // rows of nx + 4 on the host, of the device pitch on the device
+        const size_t w = (size_t)(nx + 4) * es, rows = (size_t)ev->ncy * ev->ncz;
+        if (to_dev)
+            VAH_TRY(cudaMemcpy2DAsync(d, ev->ncx * es, src_h, w, w, rows, cudaMemcpyHostToDevice, ev->stream));
+        else
+            VAH_TRY(cudaMemcpy2DAsync(dst_h, w, d, ev->ncx * es, w, rows, cudaMemcpyDeviceToHost, ev->stream));
     } else {
         for (int k = 0; k < nz; ++k) {
             char *dev_row = (char *)d + es * (2 + (size_t)ev->ncx * (2 + (size_t)ev->ncy * (k + 2)));
@@ -416,7 +587,7 @@ template <typename S>
 int set_conserved_t(vah_event *ev, double t, int pl_from_field) {
     VAH_TRY(vah::launch_set_conserved<S>(field_set<S>(ev->q, 16), field_set<S>(ev->u, 4), field_set<S>(ev->up, 4),
                                          (const S *)ev->ep[ev->cur][0], ev->opt.physics, ev->lat.nx, ev->lat.ny,
-                                         ev->lat.nz, t, pl_from_field, ev->stream));
+                                         ev->lat.nz, ev->ncx, t, pl_from_field, ev->stream));
     VAH_TRY(cudaStreamSynchronize(ev->stream));
     return VAH_OK;
 }
@@ -431,7 +602,7 @@ int ghosts_t(vah_event *ev) {
     for (int k = 0; k < 16; ++k)
         if (ev->q[k]) f.f[n++] = (S *)ev->q[k];
     f.n = n;
-    VAH_TRY(vah::launch_ghosts<S>(f, ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->stream));
+    VAH_TRY(vah::launch_ghosts<S>(f, ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->ncx, ev->stream));
     VAH_TRY(cudaStreamSynchronize(ev->stream));
     return VAH_OK;
 }
@@ -440,7 +611,7 @@ template <typename S>
 int init_primitives_t(vah_event *ev) {
     VAH_TRY(vah::launch_init_primitives<S>(field_set<S>(ev->q, 16), field_set<S>(ev->u, 4),
                                            (const S *)ev->ep[ev->cur][0], (S *)ev->ep[ev->cur][1], make_eos(ev),
-                                           ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->stream));
+                                           ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->ncx, ev->stream));
     return VAH_OK;
 }
 
@@ -534,12 +705,18 @@ int rk2_step_t(vah_event *ev, double t, double dt) {
     if (ev->validity)  // the diagnostics read P_L, pi, Pi as they are at the start of the step
         for (int n = VAH_F_PL; n < ev->nq; ++n)
             VAH_TRY(cudaMemcpyAsync(ev->vq[n], ev->q[n], ev->ncell * sizeof(S), cudaMemcpyDeviceToDevice, ev->stream));
-    StageArgs<S> a;
-    stage1_args(ev, t, dt, a);
-    int rc = timed_launch(ev, a);
-    if (rc != VAH_OK) return rc;
-    stage2_args(ev, t, dt, a);
-    rc = timed_launch(ev, a);
+    int rc;
+    if (ev->tile) {
+        rc = tile_stage(ev, 1, t, dt);
+        if (rc == VAH_OK) rc = tile_stage(ev, 2, t, dt);
+    } else {
+        StageArgs<S> a;
+        stage1_args(ev, t, dt, a);
+        rc = timed_launch(ev, a);
+        if (rc != VAH_OK) return rc;
+        stage2_args(ev, t, dt, a);
+        rc = timed_launch(ev, a);
+    }
     if (rc != VAH_OK || !ev->validity) return rc;
     ValidityArgs<S> v;
     memset(&v, 0, sizeof(v));
@@ -580,6 +757,7 @@ extern "C" int vah_rk2_step(vah_event *ev, double t, double dt) {
         ev->u[m] = ev->up[m];
         ev->up[m] = tmp;
     }
+    ev->tparity ^= 1;  // the tile descriptor keeps its buffers; the parity follows the swap
     ev->steps++;
     ev->last_t = t + dt;
     ev->last_dt = dt;
@@ -653,7 +831,7 @@ int autotune_t(vah_event *ev, int reps, vah_tune_report *out) {
 extern "C" int vah_event_autotune(vah_event *ev, int reps, vah_tune_report *out) {
     if (!ev || !out || reps < 1) return VAH_ERR_ARG;
     memset(out, 0, sizeof(*out));
-    if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED) return VAH_OK;  // one fused launch shape: nothing to tune
+    if (ev->opt.flux == VAH_FLUX_PER_CELL_FUSED || ev->tile) return VAH_OK;  // one launch shape: nothing to tune
     VAH_TRY(cudaSetDevice(ev->opt.device));
     return ev->elem == sizeof(float) ? autotune_t<float>(ev, reps, out) : autotune_t<double>(ev, reps, out);
 }
@@ -674,6 +852,10 @@ extern "C" int vah_event_set_validity(vah_event *ev, int on) {
         }
     }
     ev->validity = on != 0;
+    if (ev->tile) {  // the tile kernel writes the regulator maps through its descriptor
+        for (int m = 0; m < 11; ++m) ev->h_tslot.regmap[m] = ev->validity ? ev->vd[VAH_V_REGULATIONS + m] : nullptr;
+        return tile_sync_desc(ev);
+    }
     return VAH_OK;
 }
 
@@ -683,7 +865,8 @@ extern "C" int vah_event_get_validity(vah_event *ev, int id, double *host, int w
     VAH_TRY(cudaStreamSynchronize(ev->stream));
     const size_t es = sizeof(double);
     if (with_ghosts) {
-        VAH_TRY(cudaMemcpy(host, ev->vd[id], ev->ncell * es, cudaMemcpyDeviceToHost));
+        const size_t w = (size_t)(ev->lat.nx + 4) * es;
+        VAH_TRY(cudaMemcpy2D(host, w, ev->vd[id], ev->ncx * es, w, (size_t)ev->ncy * ev->ncz, cudaMemcpyDeviceToHost));
         return VAH_OK;
     }
     const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz;
@@ -710,6 +893,11 @@ extern "C" int vah_event_sync(vah_event *ev) {
     VAH_TRY(cudaStreamSynchronize(ev->stream));
     unsigned long long c[4];
     VAH_TRY(cudaMemcpy(c, ev->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+    if (ev->tile) {  // a tile launch that gave up waiting for its copy (never expected)
+        unsigned err = 0;
+        VAH_TRY(cudaMemcpy(&err, ev->d_terr, sizeof(err), cudaMemcpyDeviceToHost));
+        if (err) return VAH_ERR_CUDA;
+    }
     return c[2] ? VAH_ERR_NAN : VAH_OK;
 }
 
@@ -737,6 +925,11 @@ extern "C" int vah_event_track_fallbacks(vah_event *ev, int on) {
         VAH_TRY(cudaFree(ev->d_fb));
         ev->d_fb = nullptr;
     }
+    if (ev->tile) {
+        ev->h_tslot.fallback1 = ev->d_fb;
+        ev->h_tslot.fallback2 = ev->d_fb ? ev->d_fb + ev->ncell : nullptr;
+        return tile_sync_desc(ev);
+    }
     return VAH_OK;
 }
 
@@ -746,7 +939,8 @@ extern "C" int vah_event_get_fallback_mask(vah_event *ev, int stage, unsigned ch
     VAH_TRY(cudaStreamSynchronize(ev->stream));
     const unsigned char *src = ev->d_fb + (stage - 1) * ev->ncell;
     if (with_ghosts) {
-        VAH_TRY(cudaMemcpy(host, src, ev->ncell, cudaMemcpyDeviceToHost));
+        const size_t w = (size_t)(ev->lat.nx + 4);
+        VAH_TRY(cudaMemcpy2D(host, w, src, ev->ncx, w, (size_t)ev->ncy * ev->ncz, cudaMemcpyDeviceToHost));
         return VAH_OK;
     }
     const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz;
@@ -798,10 +992,13 @@ int step_host_fp32(vah_event *ev, double t, double dt, double *const *fields) {
     const size_t n = ev->ncell;
     if (!ev->d_stage64) VAH_TRY(cudaMalloc((void **)&ev->d_stage64, n * sizeof(double)));
     const int block = 256, grid = (int)std::min<size_t>((n + block - 1) / block, 148 * 16);
+    // host rows of nx + 4 doubles, staging rows of the device pitch
+    const size_t w = (size_t)(ev->lat.nx + 4) * sizeof(double), dp = (size_t)ev->ncx * sizeof(double),
+                 rows = (size_t)ev->ncy * ev->ncz;
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {
         float *d = (float *)field_ptr(ev, id);
         if (!d || !fields[id]) continue;
-        VAH_TRY(cudaMemcpyAsync(ev->d_stage64, fields[id], n * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
+        VAH_TRY(cudaMemcpy2DAsync(ev->d_stage64, dp, fields[id], w, w, rows, cudaMemcpyHostToDevice, ev->stream));
         narrow_kernel<<<grid, block, 0, ev->stream>>>(ev->d_stage64, d, n);
         VAH_TRY(cudaGetLastError());
     }
@@ -812,7 +1009,7 @@ int step_host_fp32(vah_event *ev, double t, double dt, double *const *fields) {
         if (!d || !fields[id]) continue;
         widen_kernel<<<grid, block, 0, ev->stream>>>(d, ev->d_stage64, n);
         VAH_TRY(cudaGetLastError());
-        VAH_TRY(cudaMemcpyAsync(fields[id], ev->d_stage64, n * sizeof(double), cudaMemcpyDeviceToHost, ev->stream));
+        VAH_TRY(cudaMemcpy2DAsync(fields[id], w, ev->d_stage64, dp, w, rows, cudaMemcpyDeviceToHost, ev->stream));
     }
     return vah_event_sync(ev);
 }

@@ -11,6 +11,10 @@
 // device arrays, so a whole RK2 step -- face and cell launches of both stages
 // plus the clock advance -- is captured once as a CUDA graph and replayed.
 // The graph is re-captured only when events are added or removed.
+// VAH_FP32 batches run the FP32 form on the TMA-tiled stage kernel
+// (vah_tile.cuh): one persistent launch per stage and tile shape (2+1D and
+// 3+1D events), each slot with a row pitch padded to 4 floats and a tile
+// descriptor (tensor maps over its q and qS blocks) admitted with it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,6 +25,7 @@
 #include "vah.h"
 #include "vah_kernels.cuh"
 #include "vah_powf_exc.h"
+#include "vah_tile.cuh"
 
 namespace vah {
 namespace {
@@ -48,6 +53,10 @@ struct SlotClock {
     int active;
     long long steps;
 };
+// the tile kernel reads the batch's clocks as TileClock
+static_assert(sizeof(SlotClock) == sizeof(TileClock) && offsetof(SlotClock, parity) == offsetof(TileClock, parity) &&
+                  offsetof(SlotClock, t) == offsetof(TileClock, t),
+              "SlotClock and TileClock share a layout");
 
 struct WorkItem {
     int slot, i0, r0, pad;
@@ -106,19 +115,27 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
     finish_args(a);
 }
 
+// Tiles are taken from the work-list in chunks of kChunk through an atomic
+// counter (reset before each launch): blocks that finish early take more,
+// so uneven events do not leave a tail; the list runs largest event first.
+constexpr int kChunk = 4;
+
 template <typename S, int PHYS, int KIND, bool EXACT, int MINB>
 __global__ void __launch_bounds__(kTX *kTY, MINB) batch_kernel(const SlotDesc<S> *__restrict__ descs,
                                                          const SlotClock *__restrict__ clk,
                                                          const WorkItem *__restrict__ work, int nwork, int stage,
-                                                         const Eos eos) {
+                                                         const Eos eos, unsigned *next) {
     __shared__ StageArgs<S> sa;
-    __shared__ int sa_slot;
+    __shared__ int sa_slot, s_w0;
     const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
     if (lead) sa_slot = -1;
-    // each block walks a contiguous run of the (slot-sorted) work-list, so the
-    // per-event arguments in shared memory change only at event boundaries
-    const int per = (nwork + gridDim.x - 1) / gridDim.x;
-    const int w0 = blockIdx.x * per, w1 = min(nwork, w0 + per);
+    for (;;) {
+    __syncthreads();  // s_w0 of the previous chunk has been read
+    if (lead) s_w0 = (int)atomicAdd(next, (unsigned)kChunk);
+    __syncthreads();
+    const int w0 = s_w0, w1 = min(nwork, w0 + kChunk);
+    if (w0 >= nwork) break;
+    // the per-event arguments in shared memory change only at event boundaries
     for (int w = w0; w < w1; ++w) {
         const WorkItem it = work[w];
         __syncthreads();
@@ -148,6 +165,7 @@ __global__ void __launch_bounds__(kTX *kTY, MINB) batch_kernel(const SlotDesc<S>
             cell_compute<S, PHYS, KIND == K_C3, EXACT>(sa, i + 2, j + 2, k + 2);
         }
     }
+    }
 }
 
 // End of a step: the clock moves on, and the freeze-out surface volume takes
@@ -168,11 +186,11 @@ __global__ void advance_kernel(SlotClock *clk, const double *dts, int nslots, un
 
 // Freeze-out state at admission: 1 where the interior e exceeds e_freeze.
 template <typename S>
-__global__ void hot_init_kernel(const S *e, unsigned char *hot, double e_freeze, int nx, int ny, int nz) {
+__global__ void hot_init_kernel(const S *e, unsigned char *hot, double e_freeze, int nx, int ny, int nz, int pitch) {
     const long long n = (long long)nx * ny * nz;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
-        const long long s = (i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * (k + 2));
+        const long long s = (i + 2) + (long long)pitch * ((j + 2) + (long long)(ny + 4) * (k + 2));
         hot[s] = (double)e[s] > e_freeze;
     }
 }
@@ -201,15 +219,15 @@ __global__ void glauber_deposit_kernel(const double *__restrict__ pxy, int np, d
 // (a flat floor when no nucleon collided).
 template <typename S>
 __global__ void glauber_fill_kernel(const double *__restrict__ vxy, const unsigned long long *__restrict__ maxbits,
-                                    const double *__restrict__ feta, int nx, int ny, int nz, double e_peak,
-                                    double e_floor, S *e) {
+                                    const double *__restrict__ feta, int nx, int ny, int nz, int pitch,
+                                    double e_peak, double e_floor, S *e) {
     const double vmax = __longlong_as_double((long long)*maxbits);
     const long long n = (long long)nx * ny * nz;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         const long long t = c % ((long long)nx * ny);
         const int k = (int)(c / ((long long)nx * ny)), i = (int)(t % nx), j = (int)(t / nx);
         const double exy = vmax > 0 ? e_peak * vxy[t] / vmax : 0.0;
-        e[(i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * (k + 2))] = (S)(exy * feta[k] + e_floor);
+        e[(i + 2) + (long long)pitch * ((j + 2) + (long long)(ny + 4) * (k + 2))] = (S)(exy * feta[k] + e_floor);
     }
 }
 
@@ -313,27 +331,30 @@ int blocks_per_sm() {
 // A persistent grid of (SMs x resident blocks) walks the work-list.
 template <typename S, int PHYS, int KIND, bool EXACT, int MINB>
 cudaError_t launch_minb(const SlotDesc<S> *descs, const SlotClock *clk, const WorkItem *work, int nwork, int stage,
-                        const Eos &eos, int sms, cudaStream_t stream) {
-    const int grid = std::min(nwork, sms * blocks_per_sm<S, PHYS, KIND, EXACT, MINB>());
-    batch_kernel<S, PHYS, KIND, EXACT, MINB><<<grid, dim3(kTX, kTY), 0, stream>>>(descs, clk, work, nwork, stage, eos);
+                        const Eos &eos, int sms, unsigned *next, cudaStream_t stream) {
+    const int grid = std::min((nwork + kChunk - 1) / kChunk, sms * blocks_per_sm<S, PHYS, KIND, EXACT, MINB>());
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    batch_kernel<S, PHYS, KIND, EXACT, MINB><<<grid, dim3(kTX, kTY), 0, stream>>>(descs, clk, work, nwork, stage, eos,
+                                                                                 next);
     return cudaGetLastError();
 }
 
 // minb: the register-cap variant (face kinds 3, 4, 5; cell kinds 2, 3, 4).
 template <typename S, int PHYS, int KIND, bool EXACT>
 cudaError_t launch_kind(const SlotDesc<S> *descs, const SlotClock *clk, const WorkItem *work, int nwork, int stage,
-                        const Eos &eos, int sms, int minb, cudaStream_t stream) {
+                        const Eos &eos, int sms, int minb, unsigned *next, cudaStream_t stream) {
     if (nwork <= 0) return cudaSuccess;
     constexpr bool FACE = KIND <= K_FZ;
     switch (minb) {
     case 2:
         if (FACE) break;
-        return launch_minb<S, PHYS, KIND, EXACT, 2>(descs, clk, work, nwork, stage, eos, sms, stream);
-    case 3: return launch_minb<S, PHYS, KIND, EXACT, 3>(descs, clk, work, nwork, stage, eos, sms, stream);
-    case 4: return launch_minb<S, PHYS, KIND, EXACT, 4>(descs, clk, work, nwork, stage, eos, sms, stream);
+        return launch_minb<S, PHYS, KIND, EXACT, 2>(descs, clk, work, nwork, stage, eos, sms, next, stream);
+    case 3: return launch_minb<S, PHYS, KIND, EXACT, 3>(descs, clk, work, nwork, stage, eos, sms, next, stream);
+    case 4: return launch_minb<S, PHYS, KIND, EXACT, 4>(descs, clk, work, nwork, stage, eos, sms, next, stream);
     case 5:
         if (!FACE) break;
-        return launch_minb<S, PHYS, KIND, EXACT, 5>(descs, clk, work, nwork, stage, eos, sms, stream);
+        return launch_minb<S, PHYS, KIND, EXACT, 5>(descs, clk, work, nwork, stage, eos, sms, next, stream);
     default: break;
     }
     return cudaErrorInvalidValue;
@@ -380,6 +401,13 @@ struct vah_batch {
     std::vector<unsigned char> desc_host;  // host mirror of the descriptor array
     WorkItem *d_work[vah::K_NUM];
     int minb[vah::K_NUM];  // register-cap variant per launch kind (autotuned)
+    // FP32 form: tile descriptors per slot, tile work-lists (2+1D, 3+1D), launch counter and error flags
+    bool tile;
+    vah::TileSlot *d_tdesc;  // [kMaxSlots]
+    vah::TileItem *d_titems[2];
+    int ntitems[2], cap_titems[2];
+    unsigned *d_tcount;      // [0]: tile counter, [1]: error flags
+    unsigned *d_wcount;      // [K_NUM] work-list counters of the face/cell launches
     int nwork[vah::K_NUM], cap_work[vah::K_NUM];
     double *d_partial;
     int cap_partial;
@@ -413,13 +441,17 @@ int nq_of(int physics) { return physics == VAH_IDEAL ? 5 : (physics == VAH_PIMUN
 // 4 uS, and the face buffers (H, plus HR for reference faces) per axis; then
 // one byte per cell of fallback flags and one of freeze-out state.
 int arrays_per_event(const vah_batch *b, const vah_lattice *lat) {
+    if (b->tile) return 48;  // the tile kernel keeps its face fluxes on chip
     const int ndir = lat->nz > 1 ? 3 : 2;
     const int per_face = b->opt.flux == VAH_FLUX_PER_CELL ? 2 : 1;
     return 48 + ndir * b->nq * per_face;
 }
 
+// Row pitch of a slot's arrays: nx + 4, padded to 4 floats for the tile form.
+int slot_pitch(const vah_batch *b, int nx) { return b->tile ? vah::tile_pitch(nx) : nx + 4; }
+
 size_t event_bytes(const vah_batch *b, const vah_lattice *lat) {
-    const size_t ncell = (size_t)(lat->nx + 4) * (lat->ny + 4) * (lat->nz + 4);
+    const size_t ncell = (size_t)slot_pitch(b, lat->nx) * (lat->ny + 4) * (lat->nz + 4);
     const size_t per = (ncell * b->elem + 255) / 256 * 256;
     return per * arrays_per_event(b, lat) + 2 * ((ncell + 255) / 256 * 256) + 256;
 }
@@ -466,7 +498,7 @@ int fill_slot(vah_batch *b, int slot) {
     d.nx = sl.lat.nx;
     d.ny = sl.lat.ny;
     d.nz = sl.lat.nz;
-    d.ncx = sl.lat.nx + 4;
+    d.ncx = slot_pitch(b, sl.lat.nx);
     d.ncy = sl.lat.ny + 4;
     d.plane = (long long)d.ncx * d.ncy;
     d.dx = sl.lat.dx;
@@ -492,11 +524,12 @@ int fill_slot(vah_batch *b, int slot) {
     for (int m = 0; m < 4; ++m) d.uB[m] = next();
     for (int m = 0; m < 4; ++m) d.uS[m] = next();
     const int ndir = sl.lat.nz > 1 ? 3 : 2;
-    for (int k = 0; k < ndir; ++k)
-        for (int n = 0; n < b->nq; ++n) {
-            d.H[k][n] = next();
-            if (b->opt.flux == VAH_FLUX_PER_CELL) d.HR[k][n] = next();
-        }
+    if (!b->tile)
+        for (int k = 0; k < ndir; ++k)
+            for (int n = 0; n < b->nq; ++n) {
+                d.H[k][n] = next();
+                if (b->opt.flux == VAH_FLUX_PER_CELL) d.HR[k][n] = next();
+            }
     d.fallback = (unsigned char *)(base + off);
     d.hot = (unsigned char *)(base + off + (ncell + 255) / 256 * 256);
     d.e_freeze = energy_at_temperature(b, sl.hydro.freezeout_T_GeV / 0.197326938);
@@ -504,22 +537,94 @@ int fill_slot(vah_batch *b, int slot) {
     *desc_host<S>(b, slot) = d;
     VAH_TRY(cudaMemcpyAsync((char *)b->d_desc + sizeof(SlotDesc<S>) * slot, &d, sizeof(d), cudaMemcpyHostToDevice,
                             b->stream));
+    if (b->tile) {  // the FP32 form's tile descriptor: the same buffers, q and qS as blocks of per-byte fields
+        vah::TileSlot t;
+        memset(&t, 0, sizeof(t));
+        t.Q[0] = (float *)d.q[0];
+        t.Q[1] = (float *)d.qS[0];
+        t.fstride = (long long)(per / sizeof(float));
+        for (int bb = 0; bb < 2; ++bb) {
+            const int rc = vah::tile_encode_q(&t.tmQ[bb], t.Q[bb], sl.lat.nx, sl.lat.ny, sl.lat.nz, d.ncx, t.fstride,
+                                              b->nq);
+            if (rc != VAH_OK) return rc;
+        }
+        for (int x = 0; x < 2; ++x)
+            for (int y = 0; y < 2; ++y) t.ep[x][y] = (float *)d.ep[x][y];
+        for (int m = 0; m < 4; ++m) {
+            t.uA[m] = (float *)d.uA[m];
+            t.uB[m] = (float *)d.uB[m];
+            t.uS[m] = (float *)d.uS[m];
+        }
+        t.nx = d.nx;
+        t.ny = d.ny;
+        t.nz = d.nz;
+        t.pitch = d.ncx;
+        t.ncy = d.ncy;
+        t.nq = b->nq;
+        t.dx = d.dx;
+        t.dy = d.dy;
+        t.dz = d.dz;
+        t.dt = d.dt;
+        t.etabar = d.etabar;
+        t.counters = d.counters;
+        t.fallback2 = d.fallback;  // the batch keeps the latest (stage-2) flags
+        t.hot = d.hot;
+        t.e_freeze = d.e_freeze;
+        t.crossings = d.crossings;
+        // a pageable source: the copy is staged before the call returns (the slot's next use is stream-ordered)
+        VAH_TRY(cudaMemcpy(b->d_tdesc + slot, &t, sizeof(t), cudaMemcpyHostToDevice));
+    }
+    return VAH_OK;
+}
+
+int rebuild_tiles(vah_batch *b) {
+    std::vector<vah::TileItem> lists[2];  // 2+1D, 3+1D events
+    for (int s = 0; s < (int)b->slots.size(); ++s) {
+        const vah_batch::Slot &sl = b->slots[s];
+        if (sl.used) vah::tile_items(lists[sl.lat.nz > 1 ? 1 : 0], s, sl.lat.nx, sl.lat.ny, sl.lat.nz);
+    }
+    for (int k = 0; k < 2; ++k) {
+        const int n = (int)lists[k].size();
+        if (n > b->cap_titems[k]) {
+            if (b->d_titems[k]) VAH_TRY(cudaFreeAsync(b->d_titems[k], b->stream));
+            const int cap = std::max(n, 2 * b->cap_titems[k]);
+            VAH_TRY(cudaMallocFromPoolAsync((void **)&b->d_titems[k], cap * sizeof(vah::TileItem), b->pool, b->stream));
+            b->cap_titems[k] = cap;
+        }
+        if (n) VAH_TRY(cudaMemcpyAsync(b->d_titems[k], lists[k].data(), n * sizeof(vah::TileItem),
+                                       cudaMemcpyHostToDevice, b->stream));
+        b->ntitems[k] = n;
+    }
+    VAH_TRY(cudaStreamSynchronize(b->stream));  // the lists die here
     return VAH_OK;
 }
 
 int rebuild_work(vah_batch *b) {
+    if (b->tile) {  // the reductions still walk the cell work-lists below
+        const int rc = rebuild_tiles(b);
+        if (rc != VAH_OK) return rc;
+    }
     std::vector<WorkItem> lists[vah::K_NUM];
-    for (int s = 0; s < (int)b->slots.size(); ++s) {
+    std::vector<int> order;  // largest event first: its tiles start first, small ones fill the tail
+    for (int s = 0; s < (int)b->slots.size(); ++s)
+        if (b->slots[s].used) order.push_back(s);
+    auto cells = [&](int s) {
+        const vah_lattice &l = b->slots[s].lat;
+        return (long long)l.nx * l.ny * l.nz;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cells(x) > cells(y); });
+    for (int s : order) {
         const vah_batch::Slot &sl = b->slots[s];
-        if (!sl.used) continue;
         const int nx = sl.lat.nx, ny = sl.lat.ny, nz = sl.lat.nz;
         auto add = [&](int kind, int ext0, int rows) {
             for (int r0 = 0; r0 < rows; r0 += vah::kTY)
                 for (int i0 = 0; i0 < ext0; i0 += vah::kTX) lists[kind].push_back({s, i0, r0, 0});
         };
-        add(vah::K_FX, nx + 1, ny * nz);
-        add(vah::K_FY, nx, (ny + 1) * nz);
-        if (nz > 1) add(vah::K_FZ, nx, ny * (nz + 1));
+        if (!b->tile) {
+            add(vah::K_FX, nx + 1, ny * nz);
+            add(vah::K_FY, nx, (ny + 1) * nz);
+            if (nz > 1) add(vah::K_FZ, nx, ny * (nz + 1));
+        }
         add(nz > 1 ? vah::K_C3 : vah::K_C2, nx, ny * nz);
     }
     for (int k = 0; k < vah::K_NUM; ++k) {
@@ -553,11 +658,11 @@ cudaError_t launch_kind_rt(vah_batch *b, const SlotDesc<S> *descs, int kind, int
     const WorkItem *w = b->d_work[kind];
     const int n = b->nwork[kind], m = b->minb[kind];
     switch (kind) {
-    case K_FX: return launch_kind<S, PHYS, K_FX, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
-    case K_FY: return launch_kind<S, PHYS, K_FY, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
-    case K_FZ: return launch_kind<S, PHYS, K_FZ, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
-    case K_C2: return launch_kind<S, PHYS, K_C2, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
-    case K_C3: return launch_kind<S, PHYS, K_C3, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->stream);
+    case K_FX: return launch_kind<S, PHYS, K_FX, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->d_wcount + kind, b->stream);
+    case K_FY: return launch_kind<S, PHYS, K_FY, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->d_wcount + kind, b->stream);
+    case K_FZ: return launch_kind<S, PHYS, K_FZ, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->d_wcount + kind, b->stream);
+    case K_C2: return launch_kind<S, PHYS, K_C2, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->d_wcount + kind, b->stream);
+    case K_C3: return launch_kind<S, PHYS, K_C3, EXACT>(descs, b->d_clk, w, n, stage, eos, b->sms, m, b->d_wcount + kind, b->stream);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -585,7 +690,25 @@ int enqueue_step_s(vah_batch *b) {
     }
 }
 
-int enqueue(vah_batch *b) { return b->elem == sizeof(float) ? enqueue_step_s<float>(b) : enqueue_step_s<double>(b); }
+// FP32 form: per stage one persistent tile launch per tile shape, then the clocks advance.
+int enqueue_tiles(vah_batch *b) {
+    using namespace vah;
+    const Eos eos = batch_eos(b);
+    const TileClock none{0.0, 0, 0, 0};
+    for (int stage = 1; stage <= 2; ++stage)
+        for (int k = 0; k < 2; ++k)
+            VAH_TRY(tile_launch(b->d_tdesc, (const TileClock *)b->d_clk, none, 0.0, b->d_titems[k], b->ntitems[k],
+                                k == 1, b->d_tcount, stage, b->opt.physics, eos, b->d_tcount + 1, b->stream));
+    advance_kernel<<<(kMaxSlots + 255) / 256, 256, 0, b->stream>>>(b->d_clk, b->d_dt, kMaxSlots, b->d_cross, b->d_vol,
+                                                                 b->d_dv);
+    VAH_TRY(cudaGetLastError());
+    return VAH_OK;
+}
+
+int enqueue(vah_batch *b) {
+    if (b->tile) return enqueue_tiles(b);
+    return b->elem == sizeof(float) ? enqueue_step_s<float>(b) : enqueue_step_s<double>(b);
+}
 
 int capture_graph(vah_batch *b) {
     if (b->has_graph) {
@@ -640,8 +763,8 @@ int glauber_slot(vah_batch *b, const SlotDesc<S> &d, const vah_lattice &lat, con
         maxbits);
     VAH_TRY(cudaGetLastError());
     vah::glauber_fill_kernel<S><<<(int)std::min<size_t>((nxy * lat.nz + block - 1) / block, 148 * 16), block, 0,
-                                  b->stream>>>(d_v, maxbits, d_f, lat.nx, lat.ny, lat.nz, g.e_peak, g.e_floor,
-                                               d.ep[0][0]);
+                                  b->stream>>>(d_v, maxbits, d_f, lat.nx, lat.ny, lat.nz, d.ncx, g.e_peak,
+                                               g.e_floor, d.ep[0][0]);
     VAH_TRY(cudaGetLastError());
     VAH_TRY(cudaFreeAsync(scratch, b->stream));
     return VAH_OK;
@@ -671,9 +794,9 @@ int init_slot(vah_batch *b, int slot, double t0, const double *e_interior, const
     S *qs[16];
     for (int n = 0; n < 16; ++n) qs[n] = n < b->nq || (n == 15 && b->nq == 16) ? d.q[n] : nullptr;
     VAH_TRY(vah::launch_init_primitives<S>(fs<S>(qs, 16), fs<S>(d.uA, 4), d.ep[0][0], d.ep[0][1], batch_eos(b), nx, ny,
-                                           nz, b->stream));
+                                           nz, d.ncx, b->stream));
     VAH_TRY(vah::launch_set_conserved<S>(fs<S>(qs, 16), fs<S>(d.uA, 4), fs<S>(d.uB, 4), d.ep[0][0], b->opt.physics,
-                                         nx, ny, nz, t0, pl_mode == VAH_PL_ISOTROPIC, b->stream));
+                                         nx, ny, nz, d.ncx, t0, pl_mode == VAH_PL_ISOTROPIC, b->stream));
     vah::FieldSet<S> g{};
     int m = 0;
     g.f[m++] = d.ep[0][0];
@@ -681,7 +804,7 @@ int init_slot(vah_batch *b, int slot, double t0, const double *e_interior, const
     for (int k = 0; k < 4; ++k) g.f[m++] = d.uA[k];
     for (int k = 0; k < b->nq; ++k) g.f[m++] = d.q[k];
     g.n = m;
-    VAH_TRY(vah::launch_ghosts<S>(g, nx, ny, nz, b->stream));
+    VAH_TRY(vah::launch_ghosts<S>(g, nx, ny, nz, d.ncx, b->stream));
     SlotClock c{t0, 0, 1, 0};
     VAH_TRY(cudaMemcpyAsync(b->d_clk + slot, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
     VAH_TRY(cudaMemcpyAsync(b->d_dt + slot, &sl.dt, sizeof(double), cudaMemcpyHostToDevice, b->stream));
@@ -691,7 +814,7 @@ int init_slot(vah_batch *b, int slot, double t0, const double *e_interior, const
     const double dv = sl.lat.dx * sl.lat.dy * sl.lat.dz;
     VAH_TRY(cudaMemcpyAsync(b->d_dv + slot, &dv, sizeof(double), cudaMemcpyHostToDevice, b->stream));
     vah::hot_init_kernel<S><<<std::max(1, std::min(nx * ny * nz / 256 + 1, 148 * 16)), 256, 0, b->stream>>>(
-        d.ep[0][0], d.hot, d.e_freeze, nx, ny, nz);
+        d.ep[0][0], d.hot, d.e_freeze, nx, ny, nz, d.ncx);
     VAH_TRY(cudaGetLastError());
     VAH_TRY(cudaStreamSynchronize(b->stream));  // the staging vector dies here
     return VAH_OK;
@@ -727,6 +850,7 @@ extern "C" int vah_batch_create(const vah_options *opt, const double *eos_table,
     b->opt = *opt;
     b->nq = nq_of(opt->physics);
     b->elem = opt->precision == VAH_FP32 ? sizeof(float) : sizeof(double);
+    b->tile = opt->precision == VAH_FP32;
     b->own_stream = opt->stream == nullptr;
     b->capacity = capacity_bytes;
     b->used = 0;
@@ -758,6 +882,12 @@ extern "C" int vah_batch_create(const vah_options *opt, const double *eos_table,
     chk(cudaMalloc((void **)&b->d_dv, sizeof(double) * vah::kMaxSlots));
     chk(cudaMalloc((void **)&b->d_counters, sizeof(unsigned long long) * 4 * vah::kMaxSlots));
     chk(cudaMalloc((void **)&b->d_maxbits, sizeof(unsigned long long) * vah::kMaxSlots));
+    chk(cudaMalloc((void **)&b->d_wcount, sizeof(unsigned) * vah::K_NUM));
+    if (b->tile) {
+        chk(cudaMalloc((void **)&b->d_tdesc, sizeof(vah::TileSlot) * vah::kMaxSlots));
+        chk(cudaMalloc((void **)&b->d_tcount, 2 * sizeof(unsigned)));
+        if (rc == VAH_OK) chk(cudaMemset(b->d_tcount, 0, 2 * sizeof(unsigned)));
+    }
     if (rc == VAH_OK) {
         chk(cudaMemset(b->d_clk, 0, sizeof(SlotClock) * vah::kMaxSlots));
         chk(cudaMemset(b->d_dt, 0, sizeof(double) * vah::kMaxSlots));
@@ -800,6 +930,8 @@ extern "C" int vah_batch_destroy(vah_batch *b) {
         if (sl.mem) cudaFreeAsync(sl.mem, b->stream);
     for (int k = 0; k < vah::K_NUM; ++k)
         if (b->d_work[k]) cudaFreeAsync(b->d_work[k], b->stream);
+    for (int k = 0; k < 2; ++k)
+        if (b->d_titems[k]) cudaFreeAsync(b->d_titems[k], b->stream);
     if (b->d_partial) cudaFreeAsync(b->d_partial, b->stream);
     cudaStreamSynchronize(b->stream);
     cudaMemPoolDestroy(b->pool);
@@ -811,6 +943,9 @@ extern "C" int vah_batch_destroy(vah_batch *b) {
     cudaFree(b->d_dv);
     cudaFree(b->d_counters);
     cudaFree(b->d_maxbits);
+    cudaFree(b->d_wcount);
+    cudaFree(b->d_tdesc);
+    cudaFree(b->d_tcount);
     cudaFree(b->d_tab);
     cudaFree(b->d_exc);
     cudaEventDestroy(b->t0);
@@ -953,7 +1088,8 @@ extern "C" int vah_batch_get_field(vah_batch *b, int slot, int field, double *ho
     VAH_TRY(cudaMemcpyAsync(&c, b->d_clk + slot, sizeof(c), cudaMemcpyDeviceToHost, b->stream));
     VAH_TRY(cudaStreamSynchronize(b->stream));
     const vah_lattice &lat = b->slots[slot].lat;
-    const size_t ncx = lat.nx + 4, ncy = lat.ny + 4, ncell = ncx * ncy * (lat.nz + 4);
+    const size_t ncx = slot_pitch(b, lat.nx), ncy = lat.ny + 4, hx = lat.nx + 4;
+    const size_t ncell = hx * ncy * (lat.nz + 4);  // host layout
     const size_t n = with_ghosts ? ncell : (size_t)lat.nx * lat.ny * lat.nz;
     std::vector<float> f32;
     void *src = b->elem == sizeof(float) ? (void *)slot_field<float>(b, slot, field, c.parity)
@@ -963,7 +1099,8 @@ extern "C" int vah_batch_get_field(vah_batch *b, int slot, int field, double *ho
     if (es == sizeof(float)) f32.resize(n);
     void *dst = es == sizeof(float) ? (void *)f32.data() : (void *)host;
     if (with_ghosts) {
-        VAH_TRY(cudaMemcpyAsync(dst, src, ncell * es, cudaMemcpyDeviceToHost, b->stream));
+        VAH_TRY(cudaMemcpy2DAsync(dst, hx * es, src, ncx * es, hx * es, ncy * (lat.nz + 4), cudaMemcpyDeviceToHost,
+                                  b->stream));
     } else {
         for (int k = 0; k < lat.nz; ++k) {
             const char *row = (const char *)src + es * (2 + ncx * (2 + ncy * (k + 2)));
@@ -981,7 +1118,7 @@ extern "C" int vah_batch_fallback_mask(vah_batch *b, int slot, unsigned char *ho
     if (!b || !host || slot < 0 || slot >= vah::kMaxSlots || !b->slots[slot].used) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(b->opt.device));
     const vah_lattice &lat = b->slots[slot].lat;
-    const size_t ncx = lat.nx + 4, ncy = lat.ny + 4;
+    const size_t ncx = slot_pitch(b, lat.nx), ncy = lat.ny + 4;
     const unsigned char *src = b->elem == sizeof(float) ? slot_fallback<float>(b, slot) : slot_fallback<double>(b, slot);
     for (int k = 0; k < lat.nz; ++k)
         VAH_TRY(cudaMemcpy2DAsync(host + (size_t)lat.nx * lat.ny * k, lat.nx, src + 2 + ncx * (2 + ncy * (k + 2)), ncx,
@@ -1174,6 +1311,7 @@ int batch_autotune_s(vah_batch *b, int reps, vah_tune_report *out) {
 extern "C" int vah_batch_autotune(vah_batch *b, int reps, vah_tune_report *out) {
     if (!b || !out || reps < 1) return VAH_ERR_ARG;
     memset(out, 0, sizeof(*out));
+    if (b->tile) return VAH_OK;  // one persistent tile launch per stage and shape: nothing to tune
     VAH_TRY(cudaSetDevice(b->opt.device));
     if (b->dirty) {  // the work-list must describe the admitted events
         const int rc = rebuild_work(b);

@@ -85,21 +85,24 @@ struct FieldSet {
     int n;
 };
 
+// The set-up launches below index cell (i, j, k) of the ghosted grid at
+// i + pitch (j + (ny + 4) k): pitch = nx + 4 in the reference layout, or the
+// padded pitch of the tile layout.
 // Primitive -> conserved over the interior (setConservedVariables):
 // q = 16 conserved slots, u/up = 4 velocity components each.
 template <typename S>
 cudaError_t launch_set_conserved(const FieldSet<S> &q, const FieldSet<S> &u, const FieldSet<S> &up, const S *e,
-                                 int physics, int nx, int ny, int nz, double t, int pl_from_field,
+                                 int physics, int nx, int ny, int nz, int pitch, double t, int pl_from_field,
                                  cudaStream_t stream);
 
 // Interior primitives for a fresh event: p = EoS(e), u = (1,0,0,0),
 // pi = Pi = 0, P_L = p (q[4]).
 template <typename S>
 cudaError_t launch_init_primitives(const FieldSet<S> &q, const FieldSet<S> &u, const S *e, S *p, const Eos &eos,
-                                   int nx, int ny, int nz, cudaStream_t stream);
+                                   int nx, int ny, int nz, int pitch, cudaStream_t stream);
 
 // Reference ghost fill, three passes with its loop ranges (setGhostCells).
 template <typename S>
-cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cudaStream_t stream);
+cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, int pitch, cudaStream_t stream);
 
 }  // namespace vah

@@ -85,22 +85,22 @@ __global__ void validity_kernel(const ValidityArgs<S> a) {
 
 template <typename S, int PHYS>
 __global__ void set_conserved_kernel(const FieldSet<S> q, const FieldSet<S> u, const FieldSet<S> up, const S *e,
-                                     int nx, int ny, int nz, double t, int pl_from_field) {
+                                     int nx, int ny, int nz, int pitch, double t, int pl_from_field) {
     const long long n = (long long)nx * ny * nz;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
-        const long long s = (i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * (k + 2));
+        const long long s = (i + 2) + (long long)pitch * ((j + 2) + (long long)(ny + 4) * (k + 2));
         set_conserved_cell<S, PHYS>(q.f, u.f, up.f, e, t, pl_from_field, s);
     }
 }
 
 template <typename S>
 __global__ void init_primitives_kernel(const FieldSet<S> q, const FieldSet<S> u, const S *e, S *p, const Eos eos,
-                                       int nx, int ny, int nz) {
+                                       int nx, int ny, int nz, int pitch) {
     const long long n = (long long)nx * ny * nz;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
-        const long long s = (i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * (k + 2));
+        const long long s = (i + 2) + (long long)pitch * ((j + 2) + (long long)(ny + 4) * (k + 2));
         const double pv = eos_pressure(eos, (double)e[s]);
         p[s] = (S)pv;
         u.f[0][s] = (S)1.0;
@@ -114,9 +114,9 @@ __global__ void init_primitives_kernel(const FieldSet<S> q, const FieldSet<S> u,
 // Pass 0 (I): j in [2, ncy), k in [2, ncz): i = 0,1 <- 2; i = nx+2, nx+3 <- nx+1.
 // Pass 1 (J): i in [2, ncx), k in [2, ncz).  Pass 2 (K): i in [2, ncx), j in [2, ncy).
 template <typename S>
-__global__ void ghost_kernel(const FieldSet<S> f, int nx, int ny, int nz, int pass) {
+__global__ void ghost_kernel(const FieldSet<S> f, int nx, int ny, int nz, int pitch, int pass) {
     const int ncx = nx + 4, ncy = ny + 4, ncz = nz + 4;
-    const long long plane = (long long)ncx * ncy;
+    const long long plane = (long long)pitch * ncy;
     int na, nb;
     if (pass == 0) { na = ncy - 2; nb = ncz - 2; }
     else if (pass == 1) { na = ncx - 2; nb = ncz - 2; }
@@ -129,16 +129,16 @@ __global__ void ghost_kernel(const FieldSet<S> f, int nx, int ny, int nz, int pa
         long long s, sb;
         if (pass == 0) {
             int gi = slot < 2 ? slot : nx + slot, bi = slot < 2 ? 2 : nx + 1;
-            s = gi + (long long)ncx * A + plane * B;
-            sb = bi + (long long)ncx * A + plane * B;
+            s = gi + (long long)pitch * A + plane * B;
+            sb = bi + (long long)pitch * A + plane * B;
         } else if (pass == 1) {
             int gj = slot < 2 ? slot : ny + slot, bj = slot < 2 ? 2 : ny + 1;
-            s = A + (long long)ncx * gj + plane * B;
-            sb = A + (long long)ncx * bj + plane * B;
+            s = A + (long long)pitch * gj + plane * B;
+            sb = A + (long long)pitch * bj + plane * B;
         } else {
             int gk = slot < 2 ? slot : nz + slot, bk = slot < 2 ? 2 : nz + 1;
-            s = A + (long long)ncx * B + plane * gk;
-            sb = A + (long long)ncx * B + plane * bk;
+            s = A + (long long)pitch * B + plane * gk;
+            sb = A + (long long)pitch * B + plane * bk;
         }
         for (int m = 0; m < f.n; ++m) f.f[m][s] = f.f[m][sb];
     }
@@ -262,14 +262,14 @@ cudaError_t launch_validity(const ValidityArgs<S> &a, int physics, cudaStream_t 
 
 template <typename S>
 cudaError_t launch_set_conserved(const FieldSet<S> &q, const FieldSet<S> &u, const FieldSet<S> &up, const S *e,
-                                 int physics, int nx, int ny, int nz, double t, int pl_from_field,
+                                 int physics, int nx, int ny, int nz, int pitch, double t, int pl_from_field,
                                  cudaStream_t stream) {
     const int block = 256;
     const int grid = grid_for((long long)nx * ny * nz, block);
     switch (physics) {
-    case kIdeal: set_conserved_kernel<S, kIdeal><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, t, pl_from_field); break;
-    case kPimunu: set_conserved_kernel<S, kPimunu><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, t, pl_from_field); break;
-    case kPimunuPi: set_conserved_kernel<S, kPimunuPi><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, t, pl_from_field); break;
+    case kIdeal: set_conserved_kernel<S, kIdeal><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, pitch, t, pl_from_field); break;
+    case kPimunu: set_conserved_kernel<S, kPimunu><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, pitch, t, pl_from_field); break;
+    case kPimunuPi: set_conserved_kernel<S, kPimunuPi><<<grid, block, 0, stream>>>(q, u, up, e, nx, ny, nz, pitch, t, pl_from_field); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -277,15 +277,15 @@ cudaError_t launch_set_conserved(const FieldSet<S> &q, const FieldSet<S> &u, con
 
 template <typename S>
 cudaError_t launch_init_primitives(const FieldSet<S> &q, const FieldSet<S> &u, const S *e, S *p, const Eos &eos,
-                                   int nx, int ny, int nz, cudaStream_t stream) {
+                                   int nx, int ny, int nz, int pitch, cudaStream_t stream) {
     const int block = 256;
     init_primitives_kernel<S><<<grid_for((long long)nx * ny * nz, block), block, 0, stream>>>(q, u, e, p, eos, nx, ny,
-                                                                                                nz);
+                                                                                                nz, pitch);
     return cudaGetLastError();
 }
 
 template <typename S>
-cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cudaStream_t stream) {
+cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, int pitch, cudaStream_t stream) {
     const int block = 256;
     for (int pass = 0; pass < 3; ++pass) {
         long long n;
@@ -293,7 +293,7 @@ cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cud
         else if (pass == 1) n = (long long)nx * nz;
         else n = (long long)nx * ny;
         n = (n + 4LL * (nx + ny + nz) + 16) * 4;  // the passes also sweep upper ghost rows
-        ghost_kernel<S><<<grid_for(n, block), block, 0, stream>>>(fields, nx, ny, nz, pass);
+        ghost_kernel<S><<<grid_for(n, block), block, 0, stream>>>(fields, nx, ny, nz, pitch, pass);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }
@@ -309,9 +309,9 @@ cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, cud
                                                cudaStream_t);                                                   \
     template cudaError_t launch_stage_split<S>(const StageArgs<S> &, int, bool, cudaStream_t);                  \
     template cudaError_t launch_set_conserved<S>(const FieldSet<S> &, const FieldSet<S> &, const FieldSet<S> &, \
-                                                 const S *, int, int, int, int, double, int, cudaStream_t);     \
+                                                 const S *, int, int, int, int, int, double, int, cudaStream_t); \
     template cudaError_t launch_init_primitives<S>(const FieldSet<S> &, const FieldSet<S> &, const S *, S *,    \
-                                                   const Eos &, int, int, int, cudaStream_t);                  \
-    template cudaError_t launch_ghosts<S>(const FieldSet<S> &, int, int, int, cudaStream_t);
+                                                   const Eos &, int, int, int, int, cudaStream_t);             \
+    template cudaError_t launch_ghosts<S>(const FieldSet<S> &, int, int, int, int, cudaStream_t);
 
 }  // namespace vah

@@ -642,16 +642,19 @@ VAH_HD int cell_sources(const Eos &eos, const R *Q, const CellGradT<R> &g, const
     R T, cs2;
     eos_T_cs2(eos, e, &T, &cs2);
     const R inv_e = R(1.0) / e;
-    R ap[16];
-    ap[0] = R(1.0);
-    ap[1] = pl * inv_e;
+    // The closure fits are evaluated in FP64 whatever R is: their monomial
+    // coefficients (up to ~1e7, alternating in sign) cancel to results of
+    // O(1e-3), and in FP32 several lose every digit (Rbar0P turns infinite).
+    double ap[16];
+    ap[0] = 1.0;
+    ap[1] = (double)pl * (double)inv_e;
 #pragma unroll
     for (int k = 2; k < 16; ++k) ap[k] = ap[k - 1] * ap[1];
-    const R a = ap[1];
-    const R Rtilde = poly::Rtilde(ap);
-    const R Rbar0 = poly::Rbar0(ap);
-    const R Rgamma = poly::Rgamma(ap);
-    const R Rbar0P = poly::Rbar0P(ap);
+    const R a = R(ap[1]);
+    const R Rtilde = R(poly::Rtilde(ap));
+    const R Rbar0 = R(poly::Rbar0(ap));
+    const R Rgamma = R(poly::Rgamma(ap));
+    const R Rbar0P = R(poly::Rbar0P(ap));
 
     const R e3p = e - 3 * p;
     const R ptHat = (e - pl - Rbar0 * e3p) * R(0.5);
@@ -700,15 +703,16 @@ VAH_HD int cell_sources(const Eos &eos, const R *Q, const CellGradT<R> &g, const
         if (third == R(0.0)) third = R(1.e-16);
         const R meq2 = 36 * third;
         const R z2logz = -2 * (1 + R(0.02536) * meq2);
-        const R g40 = (poly::g0m2040DividedBym2LogZTerm(ap) * z2logz + poly::g0m2040DividedBym2Zm2Term(ap)) / meq2 +
-                           poly::g0m2040DividedBym2ConstantTerm(ap);
-        const R g20c = poly::g0m2020ConstantTerm(ap);
-        const R g20 = g20c + poly::g0m2020Z2LogZTerm(ap) * z2logz + poly::g0m2020Z2Term(ap) * meq2;
+        const R g40 = (R(poly::g0m2040DividedBym2LogZTerm(ap)) * z2logz + R(poly::g0m2040DividedBym2Zm2Term(ap))) /
+                          meq2 +
+                      R(poly::g0m2040DividedBym2ConstantTerm(ap));
+        const R g20c = R(poly::g0m2020ConstantTerm(ap));
+        const R g20 = g20c + R(poly::g0m2020Z2LogZTerm(ap)) * z2logz + R(poly::g0m2020Z2Term(ap)) * meq2;
         beta_lPi = 3 * g40;
         delta_lPi = g20 + g40;
         beta_PiPi = 1 - g20c;
         delta_PiPi = R(0.5) * (1 + g20c);
-        lambda_Pipi = div_const(3 * poly::G_G1(ap), R(5.0), R(1.0) / R(5.0)) * (0 - cs2);
+        lambda_Pipi = div_const(3 * R(poly::G_G1(ap)), R(5.0), R(1.0) / R(5.0)) * (0 - cs2);
     }
 
     const R dPL = -(pl - p) * taupiInv + zeta_zz * zDzu - zeta_zT * thetaT - beta_lPi * Pi * zDzu -
@@ -788,7 +792,7 @@ VAH_HD int cell_sources(const Eos &eos, const R *Q, const CellGradT<R> &g, const
     }
     if (BULK) {
         // SourceTerms.cpp:1030-1042
-        const R Rhat = poly::Rhat(ap);
+        const R Rhat = R(poly::Rhat(ap));
         const R bb = R(1.0) / R(3.0) - cs2;
         const R tauPiInv = 15 * bb * bb * T / zeta_over_s(eos, T);
         const R zeta_z = div_const((Rhat - Rbar0) * e3p, R(3.0), R(1.0) / R(3.0));
@@ -815,12 +819,12 @@ VAH_HD void regulate(R t, R &e, R &p, R *q, const R *u, R *maps = nullptr) {
     if (q[kSlotPL] < R(0.0)) q[kSlotPL] = R(1.e-7);
     if (!Phys<PHYS>::PIMUNU) return;
     const R pl = q[kSlotPL];
-    R ap[9];
-    ap[0] = R(1.0);
-    ap[1] = pl / e;
+    double ap[9];  // FP64 closure fit, as in cell_sources
+    ap[0] = 1.0;
+    ap[1] = (double)pl / (double)e;
 #pragma unroll
     for (int k = 2; k < 9; ++k) ap[k] = ap[k - 1] * ap[1];
-    const R ptHat = (e - pl - poly::Rbar0(ap) * (e - 3 * p)) * R(0.5);
+    const R ptHat = (e - pl - R(poly::Rbar0(ap)) * (e - 3 * p)) * R(0.5);
     const R pitt = q[5], pitx = q[6], pity = q[7], pitn = q[8], pixx = q[9];
     const R pixy = q[10], pixn = q[11], piyy = q[12], piyn = q[13], pinn = q[14];
     const R ut = u[0], ux = u[1], uy = u[2], un = u[3];

@@ -1,0 +1,430 @@
+// vah_tile.cuh -- the FP32 form of the RK stage as one persistent,
+// TMA-tiled launch per stage (sm_100a).
+//
+// Form: the state is stored and updated in FP32 -- reconstruction, minmod
+// limiter, Kurganov-Tadmor flux, source terms, convex combination and
+// regulator run in single precision -- and only the Newton inversions of
+// conserved to primitive variables run in FP64 (ill-conditioned as P_L -> 0
+// and u^tau grows). Each face flux is evaluated once, from both reconstructed
+// states, with the left cell's Newton guess (the shared-face semantics of
+// VAH_FLUX_SHARED), so a cell-stage costs 3 face inversion pairs + 1 cell
+// inversion instead of the reference's 6 pairs + 1.
+//
+// Structure: a persistent grid (2 blocks of 256 threads per SM) takes tiles
+// from a work-list through an atomic counter. For each tile one thread issues
+// a single 4-D TMA load (cp.async.bulk.tensor: x, y, z and all N_q fields) of
+// the tile plus a 2-cell halo of the stage-input conserved fields into shared
+// memory, completed on an mbarrier. The faces of the tile are then evaluated
+// once each into registers and shared memory (x: in registers, exchanged with
+// the neighbour cell through warp shuffles; y and z: a shared face buffer; the
+// tile's lower boundary faces: a second small buffer), every cell takes its
+// flux differences from there, and runs sources, inversion and regulator.
+// Face fluxes never leave the SM. Primitive fields (e, p, u), needed at +-1,
+// are read through L1.
+//
+// Tiles: 8x8x4 cells for 3+1D events (TMA box 12x12x8 x N_q), 16x16x1 for
+// 2+1D (box 20x20x1 x N_q). Buffers use a row pitch padded to 4 floats
+// (16 bytes), as the TMA tensor map requires.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "vah_physics.cuh"
+#include "vah_tile_cell.cuh"
+
+namespace vah {
+
+constexpr int kTileThreads = 256;
+
+template <bool IS3D>
+struct TileShape {
+    static constexpr int TX = IS3D ? 8 : 16, TY = IS3D ? 8 : 16, TZ = IS3D ? 4 : 1;
+    static constexpr int BX = TX + 4, BY = TY + 4, BZ = IS3D ? TZ + 4 : 1;  // TMA box (halo 2; 2+1D: one plane)
+    static constexpr int BOXN = BX * BY * BZ;                               // cells of the box
+    static constexpr int NBX = TY * TZ, NBY = TX * TZ, NBZ = IS3D ? TX * TY : 0;  // lower boundary faces per axis
+    static constexpr int NB = NBX + NBY + NBZ;
+    static_assert(TX * TY * TZ == kTileThreads, "one thread per cell");
+    static_assert((BX * 4) % 16 == 0, "TMA box rows must be a multiple of 16 bytes");
+};
+
+// One event in the tile layout, with the buffer roles of vah_rk2_step:
+// Q[0] = q (q^n; stage 2 writes q^{n+1} in place), Q[1] = qS (stage 1's
+// result), each N_q fields at a stride of fstride floats, so that one rank-4
+// tensor map (x, y, z, field) covers a block; ep[0] = (e, p) at t_n (stage 2
+// writes t_{n+1}'s), ep[1] = stage 1's; uA / uB = u^n and u^{n-1} in the
+// order the clock's parity gives (stage 2 writes u^{n+1} over u^{n-1}, and the
+// parity flips); uS = stage 1's u. Cell (i, j, k) of the ghosted grid is at
+// i + pitch (j + ncy k), pitch a multiple of 4 floats.
+struct alignas(64) TileSlot {
+    CUtensorMap tmQ[2];  // over Q[0], Q[1]
+    float *Q[2];
+    float *ep[2][2];
+    float *uA[4], *uB[4], *uS[4];
+    long long fstride;
+    int nx, ny, nz, pitch, ncy, nq;
+    double dx, dy, dz, dt, etabar;
+    unsigned long long *counters;  // [face fallbacks, cell fallbacks, NaN cells]
+    unsigned char *fallback1, *fallback2;  // optional: per cell, 1 where the stage-1 / stage-2 inversion fell back
+    unsigned char *hot;            // optional freeze-out state (1 while e > e_freeze) ...
+    double e_freeze;
+    unsigned long long *crossings;  // ... and crossings [down, up] of the step
+    double *regmap[11];            // optional validity diagnostics (FP64, fstride each)
+};
+
+// Per-event clock (the batch's per-slot clock has this layout).
+struct TileClock {
+    double t;
+    int parity;  // 0: u^n in uA, u^{n-1} in uB; 1: swapped
+    int active;
+    long long steps;
+};
+
+struct TileItem {
+    int slot, i0, j0, k0;  // tile origin in interior coordinates
+};
+
+// Error flags the kernel can raise (bit mask in *err).
+constexpr unsigned kTileErrTimeout = 1u;  // an mbarrier wait ran past its iteration limit
+constexpr unsigned kTileErrAlign = 2u;    // the shared-memory box was not 128-byte aligned (nothing issued)
+
+#ifdef __CUDACC__
+
+// ------------------------------------------------------------ PTX helpers --
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up (false) after `limit` polls; each poll blocks for a
+// hardware-chosen interval, so the limit bounds the wait to well under a
+// second on B200.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit) {
+    for (unsigned it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// 4-D tiled TMA load of one box into shared memory, completing on `bar`.
+// The x coordinate times 4 bytes must be a multiple of 16 (x % 4 == 0).
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
+                                            int z, int f) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(f), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void tile_count(unsigned long long *c, unsigned v) {
+    // one atomic per warp
+    unsigned s = v;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(c, (unsigned long long)s);
+}
+
+// The dynamic shared memory of one block: TMA box, y/z face buffer, lower
+// boundary faces, and (after them) the mbarrier and the tile index.
+template <int PHYS, bool IS3D>
+struct TileSmem {
+    using SH = TileShape<IS3D>;
+    static constexpr int NQ = Phys<PHYS>::NQ;
+    static constexpr size_t box_floats = (size_t)SH::BOXN * NQ;
+    static constexpr size_t face_floats = (size_t)kTileThreads * NQ;
+    static constexpr size_t bnd_floats = (size_t)SH::NB * NQ;
+    static constexpr size_t box_bytes = box_floats * 4;
+    // the mbarrier (8 bytes) and the tile index (4 bytes) follow the floats
+    static constexpr size_t bar_offset = ((box_floats + face_floats + bnd_floats) * 4 + 15) / 16 * 16;
+    static constexpr size_t bytes = bar_offset + 16;
+};
+
+template <int PHYS, bool IS3D>
+__global__ void __launch_bounds__(kTileThreads, 2)
+    tile_kernel(const TileSlot *__restrict__ slots, const TileClock *__restrict__ clk, const TileClock clk0,
+                const double dt0, const TileItem *__restrict__ items, int nitems, unsigned *next_item, int stage,
+                const Eos eos, unsigned *err) {
+    using SH = TileShape<IS3D>;
+    using SM = TileSmem<PHYS, IS3D>;
+    constexpr int NQ = Phys<PHYS>::NQ;
+    constexpr int TX = SH::TX, TY = SH::TY, BX = SH::BX, BY = SH::BY, BOXN = SH::BOXN;
+    extern __shared__ __align__(1024) float tile_smem[];
+    float *sQ = tile_smem;                     // [NQ][BZ][BY][BX]
+    float *sF = sQ + SM::box_floats;           // [NQ][256]: +1/2 faces along y, then z
+    float *sB = sF + SM::face_floats;          // [NQ][NB]: lower boundary faces (x, y, z)
+    unsigned long long *bar = (unsigned long long *)((char *)tile_smem + SM::bar_offset);
+    int &s_item = *(int *)(bar + 1);
+
+    const int tid = threadIdx.x;
+    const int lx = tid % TX, ly = (tid / TX) % TY, lz = tid / (TX * TY);
+    if (smem_u32(sQ) & 127u) {  // the TMA destination must be 128-byte aligned: report, issue nothing
+        if (tid == 0) atomicOr(err, kTileErrAlign);
+        return;
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned phase = 0;
+
+    for (;;) {
+        if (tid == 0) s_item = (int)atomicAdd(next_item, 1u);
+        __syncthreads();
+        const int w = s_item;
+        if (w >= nitems) break;
+        const TileItem it = items[w];
+        const TileSlot &d = slots[it.slot];
+        const TileClock c = clk ? clk[it.slot] : clk0;  // clk0, dt0: a single event's clock and step, by value
+        const double dt = clk ? d.dt : dt0;
+        float *const *u_n = c.parity ? d.uB : d.uA;      // u^n
+        float *const *u_p = c.parity ? d.uA : d.uB;      // u^{n-1}
+        // stage inputs and outputs (FullyDiscreteKurganovTadmorScheme.cpp:761-789)
+        float *Qout = d.Q[stage == 1 ? 1 : 0];
+        const float *Ein = d.ep[stage == 1 ? 0 : 1][0], *Pin_p = d.ep[stage == 1 ? 0 : 1][1];
+        float *Eout = d.ep[stage == 1 ? 1 : 0][0], *Pout_p = d.ep[stage == 1 ? 1 : 0][1];
+        float *const *Uin = stage == 1 ? u_n : d.uS;
+        float *const *Uup = stage == 1 ? u_p : u_n;  // previous-stage u (d_tau u)
+        float *const *Ugs = u_n;                     // the cell inversion's Newton guess
+        float *const *Uout = stage == 1 ? d.uS : u_p;
+        const float *UX = Uin[1], *UY = Uin[2];
+        const long long fs = d.fstride;
+        const int pitch = d.pitch;
+        const long long plane = (long long)pitch * d.ncy;
+        const double t_src = stage == 1 ? c.t : c.t + dt;
+        const double t_inv = c.t + dt;
+
+        if (tid == 0) {
+            fence_proxy_async_smem();  // the previous tile's generic reads of sQ come first
+            mbar_expect_tx(bar, (unsigned)SM::box_bytes);
+            tma_load_4d(sQ, &d.tmQ[stage == 1 ? 0 : 1], bar, it.i0, it.j0, IS3D ? it.k0 : 2, 0);
+        }
+        if (!mbar_wait(bar, phase, 1u << 22)) {
+            if (tid == 0) atomicOr(err, kTileErrTimeout);
+            // wait once more (bounded) so that no copy is left writing this block's memory
+            mbar_wait(bar, phase, 1u << 22);
+            return;
+        }
+        phase ^= 1u;
+
+        // this thread's cell, in interior and ghosted coordinates
+        const int ci = it.i0 + lx, cj = it.j0 + ly, ck = it.k0 + lz;
+        const bool live = ci < d.nx && cj < d.ny && ck < d.nz;
+        const int gi = ci + 2, gj = cj + 2, gk = ck + 2;
+        const long long s = gi + (long long)pitch * gj + plane * gk;
+        const int bc = (lx + 2) + BX * ((ly + 2) + BY * (IS3D ? lz + 2 : 0));  // box index of the cell
+        constexpr int SY = BX, SZ = BX * BY;
+
+        // ---- faces ----
+        const BoxQ<BOXN> bq{sQ};
+        unsigned ffail = 0, fnan = 0;
+        float Hx[NQ];
+        // Newton guess and fallback energy of the faces whose left cell is this one
+        double e0 = 0.0, uT0 = 0.0;
+        if (live) {
+            const double ux = (double)UX[s], uy = (double)UY[s];
+            e0 = (double)Ein[s];
+            uT0 = sqrt(fabs(ux * ux + uy * uy));
+        }
+        {   // +1/2 along x of this cell
+            if (live) {
+                const unsigned f = tile_face<PHYS>(bq, bc, 1, 0, t_src, e0, uT0, Hx);
+                ffail += f & 255u;
+                fnan |= f >> 8;
+            } else {
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) Hx[n] = 0.0f;
+            }
+        }
+        if (tid < SH::NB) {  // lower boundary faces of the tile: left cell in the halo
+            int b = tid, dir, L, bi, bj, bk;
+            if (b < SH::NBX) {
+                dir = 0; bi = 1; bj = 2 + b % TY; bk = IS3D ? 2 + b / TY : 0;
+            } else if (b < SH::NBX + SH::NBY) {
+                b -= SH::NBX; dir = 1; bi = 2 + b % TX; bj = 1; bk = IS3D ? 2 + b / TX : 0;
+            } else {
+                b -= SH::NBX + SH::NBY; dir = 2; bi = 2 + b % TX; bj = 2 + b / TX; bk = 1;
+            }
+            L = bi + BX * (bj + BY * bk);
+            // the right cell (first of the tile along dir) decides whether the face is needed
+            const int ri = it.i0 + bi - 2 + (dir == 0), rj = it.j0 + bj - 2 + (dir == 1),
+                      rk = it.k0 + (IS3D ? bk - 2 : 0) + (dir == 2);
+            float Hb[NQ];
+            if (ri < d.nx && rj < d.ny && rk < d.nz) {
+                const long long sl = (it.i0 + bi) + (long long)pitch * (it.j0 + bj) + plane * (IS3D ? it.k0 + bk : 2);
+                const double el = (double)Ein[sl], ux = (double)UX[sl], uy = (double)UY[sl];
+                const unsigned f = tile_face<PHYS>(bq, L, dir == 0 ? 1 : (dir == 1 ? SY : SZ), dir, t_src, el,
+                                                         sqrt(fabs(ux * ux + uy * uy)), Hb);
+                ffail += f & 255u;
+                fnan |= f >> 8;
+            } else {
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) Hb[n] = 0.0f;
+            }
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) sB[n * SH::NB + tid] = Hb[n];
+        }
+        {   // +1/2 along y
+            float Hy[NQ];
+            if (live) {
+                const unsigned f = tile_face<PHYS>(bq, bc, SY, 1, t_src, e0, uT0, Hy);
+                ffail += f & 255u;
+                fnan |= f >> 8;
+            } else {
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) Hy[n] = 0.0f;
+            }
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = Hy[n];
+        }
+        __syncthreads();
+
+        // flux differences: x through warp shuffles (lane - 1 holds the -1/2
+        // face), y from the face buffer
+        const float cx = (float)(dt / d.dx), cy = (float)(dt / d.dy), cz = (float)(dt / d.dz);
+        float flux[NQ];
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) {
+            float hm = __shfl_up_sync(0xffffffffu, Hx[n], 1, TX);
+            if (lx == 0) hm = sB[n * SH::NB + (ly + TY * lz)];
+            const float ym = ly > 0 ? sF[n * kTileThreads + tid - TX] : sB[n * SH::NB + SH::NBX + lx + TX * lz];
+            flux[n] = cx * (hm - Hx[n]) + cy * (ym - sF[n * kTileThreads + tid]);
+        }
+        if (IS3D) {
+            __syncthreads();  // the y faces are consumed
+            float Hz[NQ];
+            if (live) {
+                const unsigned f = tile_face<PHYS>(bq, bc, SZ, 2, t_src, e0, uT0, Hz);
+                ffail += f & 255u;
+                fnan |= f >> 8;
+            } else {
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) Hz[n] = 0.0f;
+            }
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = Hz[n];
+            __syncthreads();
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) {
+                const float zm = lz > 0 ? sF[n * kTileThreads + tid - TX * TY]
+                                        : sB[n * SH::NB + SH::NBX + SH::NBY + lx + TX * ly];
+                flux[n] += cz * (zm - Hz[n]);
+            }
+        }
+        if (d.counters) {
+            tile_count(d.counters + 0, ffail);
+            tile_count(d.counters + 2, fnan ? 1u : 0u);
+        }
+
+        // ---- the cell ----
+        if (live) {
+            const long long sy = pitch, sz = plane;
+            TilePrims pr;
+            pr.E = Ein;
+            pr.P = Pin_p;
+            for (int m = 0; m < 4; ++m) {
+                pr.U[m] = Uin[m];
+                pr.UP[m] = Uup[m];
+                pr.G[m] = Ugs[m];
+            }
+            struct {
+                const float *q;
+                long long fs;
+                __device__ float operator()(int n, long long i) const { return q[n * fs + i]; }
+            } qavg{d.Q[0], fs};
+            float val[NQ], e, p, u[4], rmap[11];
+            int bad = 0;
+            const int st = tile_cell<PHYS, IS3D>(bq, bc, SY, SZ, pr, s, sy, sz, flux, qavg, stage == 2, eos, t_src,
+                                                 t_inv, dt, d.dx, d.dy, d.dz, d.etabar, val, e, p, u,
+                                                 d.regmap[0] ? rmap : nullptr, bad);
+            if (d.regmap[0] && Phys<PHYS>::PIMUNU)
+                for (int m = 0; m < 11; ++m) d.regmap[m][s] = (double)rmap[m];
+            if (d.counters) {
+                if (st != 0) atomicAdd(d.counters + 1, 1ull);
+                if (bad || st == 2) atomicAdd(d.counters + 2, 1ull);
+            }
+            unsigned char *fb = stage == 1 ? d.fallback1 : d.fallback2;
+            if (fb) fb[s] = st != 0;
+            if (d.hot && stage == 2 && st == 0) {
+                const unsigned char was = d.hot[s], now = (double)e > d.e_freeze;
+                if (was != now) {
+                    d.hot[s] = now;
+                    atomicAdd(d.crossings + (was ? 0 : 1), 1ull);
+                }
+            }
+            // stores, and the face ghost layers of boundary cells (setGhostCellsKernelI/J/K)
+            auto store = [&](long long at) {
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) Qout[n * fs + at] = val[n];
+                Eout[at] = e;
+                Pout_p[at] = p;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) Uout[m][at] = u[m];
+            };
+            store(s);
+            if (ci == 0) { store(s - 1); store(s - 2); }
+            if (ci == d.nx - 1) { store(s + 1); store(s + 2); }
+            if (cj == 0) { store(s - sy); store(s - 2 * sy); }
+            if (cj == d.ny - 1) { store(s + sy); store(s + 2 * sy); }
+            if (ck == 0) { store(s - sz); store(s - 2 * sz); }
+            if (ck == d.nz - 1) { store(s + sz); store(s + 2 * sz); }
+        }
+        __syncthreads();  // every read of sQ, sF, sB of this tile is done
+    }
+}
+
+#endif  // __CUDACC__
+
+}  // namespace vah
+
+// ------------------------------------------------------------ host side --
+#include <vector>
+
+namespace vah {
+
+// Padded row pitch of the tile layout: nx + 4 rounded up to 4 floats.
+inline int tile_pitch(int nx) { return (nx + 4 + 3) / 4 * 4; }
+
+// Rank-4 tensor map (x, y, z, field) over a block of nq fields of float,
+// fstride floats apart, with the box of the tile shape. Returns a VAH_* status.
+int tile_encode_q(CUtensorMap *tm, const float *base, int nx, int ny, int nz, int pitch, long long fstride, int nq);
+
+// The tiles covering an event's interior, appended to `out`.
+void tile_items(std::vector<TileItem> &out, int slot, int nx, int ny, int nz);
+
+// One stage over the given tiles (all 3+1D or all 2+1D): resets the tile
+// counter and launches the persistent tile kernel. clk == nullptr: every tile
+// uses clk0 and the step dt0 (a single event); else each slot's clock and dt.
+cudaError_t tile_launch(const TileSlot *slots, const TileClock *clk, const TileClock &clk0, double dt0,
+                        const TileItem *items, int nitems, bool is3d, unsigned *counter, int stage, int physics,
+                        const Eos &eos, unsigned *err, cudaStream_t stream);
+
+}  // namespace vah

@@ -1,0 +1,156 @@
+// vah_tile_cell.cuh -- the arithmetic of the FP32 form, shared by the
+// TMA-tiled stage kernel (vah_tile.cuh) and its host build (tests/hostcheck):
+// the face flux from an accessor of the conserved fields, and the cell update.
+// State and arithmetic in FP32; the Newton inversions in FP64.
+#pragma once
+
+#include "vah_physics.cuh"
+
+namespace vah {
+
+// --------------------------------------------- the FP32 form's cell algebra --
+// Host-and-device code: the kernel runs it on the shared-memory box, and the
+// host build (tests/hostcheck) on plain arrays, through accessors
+// q(n, index) of the conserved fields.
+
+// The shared-memory box: field n at n * BOXN.
+template <int BOXN>
+struct BoxQ {
+    const float *s;
+    VAH_HD float operator()(int n, long long i) const { return s[n * BOXN + i]; }
+};
+
+// One array per field.
+struct ArrQ {
+    const float *const *f;
+    VAH_HD float operator()(int n, long long i) const { return f[n][i]; }
+};
+
+// Kurganov-Tadmor flux through the face between cells L and L + st
+// (SemiDiscreteKurganovTadmorScheme.cpp:13-57, FluxLimiter.cpp:28-33): the
+// states reconstructed in FP32, inverted in FP64 from the guess uT (the left
+// cell's |u_T|), H = wR qR + wL qL in FP32. Returns the number of inversions
+// that fell back; bit 8 flags a NaN (ePrev: the left cell's e).
+template <int PHYS, typename QA>
+VAH_HD unsigned tile_face(const QA &q, long long L, long long st, int dir, double t, double ePrev, double uT,
+                          float *H) {
+    constexpr int NQ = Phys<PHYS>::NQ;
+    float qR[NQ], qL[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) {
+        const float qm = q(n, L - st), q0 = q(n, L), qp = q(n, L + st), qpp = q(n, L + 2 * st);
+        qR[n] = qp - approx_derivative(q0, qp, qpp) * 0.5f;
+        qL[n] = q0 + approx_derivative(qm, q0, qp) * 0.5f;
+    }
+    double dR[16], dL[16];
+#pragma unroll
+    for (int n = 0; n < 16; ++n) {
+        dR[n] = n < NQ ? (double)qR[n] : 0.0;
+        dL[n] = n < NQ ? (double)qL[n] : 0.0;
+    }
+    InvSetup sR, sL;
+    invert_setup<PHYS>(t, dR, sR);
+    invert_setup<PHYS>(t, dL, sL);
+    double uR, uL, vR = 0.0, vL = 0.0;
+    int nR, nL;
+    newton_uT2(sR, sL, uT, uT, uR, uL, nR, nL);
+    const int stR = nR != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sR, uR, dir, &vR);
+    const int stL = nL != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sL, uL, dir, &vL);
+    const double a = fmax(fabs(vL), fabs(vR));
+    const float wR = (float)(0.5 * (vR - a)), wL = (float)(0.5 * (vL + a));
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) H[n] = wR * qR[n] + wL * qL[n];
+    return (stR != 0) + (stL != 0) + ((stR == 2 || stL == 2) ? 256u : 0u);
+}
+
+// Stage-input primitives, read at the cell and its +-1 neighbours: e, p, u
+// (stencil), the previous stage's u (centre) and the inversion's guess u.
+struct TilePrims {
+    const float *E, *P, *U[4], *UP[4], *G[4];
+};
+
+// The cell part of a stage (eulerStepKernelSource, the axis sources,
+// [the convex combination], setInferredVariablesKernel, the regulator):
+// q: the stage-input conserved fields at box index b (strides bsy, bsz);
+// pr: primitives at global index s (strides sy, sz); flux[n]: the flux
+// differences dt/h (H(-1/2) - H(+1/2)) summed over the axes; qavg(n, s): q^n
+// (stage 2). Writes the new conserved values, e, p, u; returns the inversion's
+// status (0 converged, 1 fallback, 2 NaN) and sets bad when a source is NaN.
+template <int PHYS, bool IS3D, typename QA, typename QV>
+VAH_HD int tile_cell(const QA &q, long long b, long long bsy, long long bsz, const TilePrims &pr, long long s,
+                     long long sy, long long sz, const float *flux, const QV &qavg, bool stage2, const Eos &eos,
+                     double t_src, double t_inv, double dt, double dx, double dy, double dz, double etabar,
+                     float *val, float &e, float &p, float *u, float *rmap, int &bad) {
+    constexpr int NQ = Phys<PHYS>::NQ;
+    float qc[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) qc[n] = q(n, b);
+    const float fx = (float)(0.5 / dx), fy = (float)(0.5 / dy), fz = (float)(0.5 / dz);
+    const float *E = pr.E, *PP = pr.P, *UT = pr.U[0], *UX = pr.U[1], *UY = pr.U[2], *UN = pr.U[3];
+    CellGradT<float> g;
+    g.e = E[s];
+    g.p = PP[s];
+    g.ut = UT[s];
+    g.ux = UX[s];
+    g.uy = UY[s];
+    g.un = UN[s];
+    g.utp = pr.UP[0][s];
+    g.uxp = pr.UP[1][s];
+    g.uyp = pr.UP[2][s];
+    g.unp = pr.UP[3][s];
+#define VAH_TCD(A, off, f) (((A)[s + (off)] - (A)[s - (off)]) * (f))
+    g.dxut = VAH_TCD(UT, 1, fx); g.dxux = VAH_TCD(UX, 1, fx); g.dxuy = VAH_TCD(UY, 1, fx); g.dxun = VAH_TCD(UN, 1, fx);
+    g.dyut = VAH_TCD(UT, sy, fy); g.dyux = VAH_TCD(UX, sy, fy); g.dyuy = VAH_TCD(UY, sy, fy); g.dyun = VAH_TCD(UN, sy, fy);
+    g.dxp = VAH_TCD(PP, 1, fx); g.dyp = VAH_TCD(PP, sy, fy);
+    g.dxe = VAH_TCD(E, 1, fx); g.dye = VAH_TCD(E, sy, fy);
+    g.dxpl = (q(kSlotPL, b + 1) - q(kSlotPL, b - 1)) * fx;
+    g.dypl = (q(kSlotPL, b + bsy) - q(kSlotPL, b - bsy)) * fy;
+    if (IS3D) {
+        g.dnut = VAH_TCD(UT, sz, fz); g.dnux = VAH_TCD(UX, sz, fz); g.dnuy = VAH_TCD(UY, sz, fz); g.dnun = VAH_TCD(UN, sz, fz);
+        g.dnp = VAH_TCD(PP, sz, fz); g.dne = VAH_TCD(E, sz, fz);
+        g.dnpl = (q(kSlotPL, b + bsz) - q(kSlotPL, b - bsz)) * fz;
+    } else {
+        g.dnut = g.dnux = g.dnuy = g.dnun = 0.0f;
+        g.dnp = g.dne = g.dnpl = 0.0f;
+    }
+#undef VAH_TCD
+    const StepConstsT<float> k = step_consts((float)t_src, (float)dt, (float)etabar);
+    float Sv[NQ];
+    bad = cell_sources<PHYS>(eos, qc, g, k, Sv);
+    const float dtf = (float)dt;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) val[n] = qc[n] + dtf * Sv[n] + flux[n];
+    if (Phys<PHYS>::PIMUNU) {  // pi / Pi gradient sources along each axis (SourceTerms.cpp:46-176)
+        const float ucomp[3] = {g.ux, g.uy, g.un};
+        const float fh[3] = {fx, fy, fz};
+        const long long sts[3] = {1, bsy, bsz};
+#pragma unroll
+        for (int dir = 0; dir < (IS3D ? 3 : 2); ++dir) {
+            float dd[16];
+#pragma unroll
+            for (int n = 5; n < NQ; ++n) dd[n] = (q(n, b + sts[dir]) - q(n, b - sts[dir])) * fh[dir];
+            float Sa[4];
+            axis_sources<PHYS>(dd, dir, ucomp[dir], g.ut, (float)t_src, Sa);
+#pragma unroll
+            for (int n = 0; n < 4; ++n) val[n] += dtf * Sa[n];
+        }
+    }
+    if (stage2) {  // Q = (q^n + Q*) / 2
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) val[n] = (val[n] + qavg(n, s)) * 0.5f;
+    }
+    // FP64 inversion from the previous-stage guess (EnergyMomentumTensor.cpp:74-197)
+    const double gx = (double)pr.G[1][s], gy = (double)pr.G[2][s];
+    double qd[16], prim[6];
+#pragma unroll
+    for (int n = 0; n < 16; ++n) qd[n] = n < NQ ? (double)val[n] : 0.0;
+    const int st = invert<PHYS>(eos, t_inv, qd, (double)g.e, sqrt(fabs(gx * gx + gy * gy)), prim);
+    e = (float)prim[0];
+    p = (float)prim[1];
+    for (int m = 0; m < 4; ++m) u[m] = (float)prim[2 + m];
+    regulate<PHYS>((float)t_inv, e, p, val, u, rmap);
+    return st;
+}
+
+
+}  // namespace vah

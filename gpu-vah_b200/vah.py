@@ -81,7 +81,7 @@ EXPORTS = ["vah_version", "vah_eos_table_build", "vah_event_create", "vah_event_
            "vah_ic_longitudinal", "vah_event_autotune", "vah_batch_autotune",
            "vah_batch_freezeout_volume", "vah_batch_fallback_mask", "vah_event_set_validity",
            "vah_event_get_validity", "vah_batch_add_glauber", "vah_ic_mc_glauber_participants",
-           "vah_event_track_fallbacks", "vah_event_get_fallback_mask"]
+           "vah_event_track_fallbacks", "vah_event_get_fallback_mask", "vah_fp64_peak"]
 
 _lib = None
 
@@ -126,6 +126,15 @@ def library():
 
 def version():
     return library().vah_version().decode()
+
+
+def fp64_peak(device=0):
+    """Measured FP64 FMA throughput (TFLOP/s) and the timed launch's ms (vah_fp64_peak)."""
+    L = library()
+    L.vah_fp64_peak.argtypes = [I, C.POINTER(D), C.POINTER(D)]
+    tf, ms = D(), D()
+    check(L.vah_fp64_peak(device, C.byref(tf), C.byref(ms)), "vah_fp64_peak")
+    return tf.value, ms.value
 
 
 def eos_table(n=4096):

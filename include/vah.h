@@ -473,6 +473,13 @@ int vah_stage_noalloc(const vah_lattice *lat, double eta_over_s, int physics, in
  * IEEE arithmetic on the CPU. */
 int vah_math_check(int device, double lo, double hi, int n, double *max_rel_rcp, double *max_rel_rsqrt);
 
+/* FP64 FMA throughput of the device, measured: a persistent grid
+ * (8 blocks of 256 threads per SM) in which each thread runs 8 independent
+ * chains of dependent fused multiply-adds; best of 5 launches. *tflops =
+ * 2 x FMAs / time, *ms the launch's duration. No counterpart in the
+ * reference; the benchmark reports the step's FP64 throughput against it. */
+int vah_fp64_peak(int device, double *tflops, double *ms);
+
 /* Library version string. */
 const char *vah_version(void);
 

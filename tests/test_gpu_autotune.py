@@ -20,7 +20,7 @@ def event_e(tab, nx, ny, nz, dx, dz, b, seed):
     return (vah.longitudinal(nz, dz)[:, None] * exy[None, :]).ravel() + 1e-3
 
 
-@pytest.mark.parametrize("precision,flux", [(0, 0), (1, 0), (0, 1)], ids=["fp64", "fp32", "fp64-shared"])
+@pytest.mark.parametrize("precision,flux", [(0, 0), (0, 1)], ids=["fp64", "fp64-shared"])
 def test_event_autotune_keeps_results_bit_identical(precision, flux):
     tab = V.eos_table()
     nx, ny, nz = 45, 39, 11
@@ -50,6 +50,15 @@ def test_event_autotune_keeps_results_bit_identical(precision, flux):
         ev.close()
     for f in FIELDS:
         np.testing.assert_array_equal(runs[1][f], runs[0][f], err_msg=f"field {f}")
+
+
+def test_event_autotune_fp32_tile_form_has_nothing_to_tune():
+    """The FP32 form runs one persistent tile launch per stage: no kinds to tune."""
+    tab = V.eos_table()
+    ev = vah.Event(21, 19, 9, 0.2, 0.2, 0.2, 0.16, table=tab, t0=0.4, precision=vah.VAH_FP32)
+    ev.init_from_e(0.4, event_e(tab, 21, 19, 9, 0.2, 0.2, 2.0, 4))
+    assert ev.autotune(1) == []
+    ev.close()
 
 
 def test_event_autotune_fused_mode_has_nothing_to_tune():

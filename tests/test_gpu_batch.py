@@ -34,14 +34,17 @@ def rel(a, b, floor=0.0):
     return 0.0 if d == 0 else d / max(np.max(np.abs(b)), floor)
 
 
-@pytest.mark.parametrize("flux", [0, 1], ids=["reference_faces", "shared_faces"])
-def test_event_alone_and_in_the_mix_agree(flux):
+@pytest.mark.parametrize("precision,flux", [(0, 0), (0, 1), (1, 0)],
+                         ids=["reference_faces", "shared_faces", "fp32_tile"])
+def test_event_alone_and_in_the_mix_agree(precision, flux):
     """Each event gives bit-identical results alone in a batch and mixed with
     the others (same kernels, per-event arithmetic only), and agrees with the
-    single-event path to 1e-12 (a separately compiled kernel: FMA contraction
-    may differ in the last bit)."""
+    single-event path to 1e-12 in FP64 (a separately compiled kernel: FMA
+    contraction may differ in the last bit) and 1e-5 in the FP32 form (the
+    same tile kernel; the batch's clock adds dt step by step where the event
+    path computes t0 + n dt, which moves the last bit of FP32 arithmetic)."""
     tab = V.eos_table()
-    mixed = vah.Batch(table=tab, flux=flux)
+    mixed = vah.Batch(table=tab, flux=flux, precision=precision)
     inputs = []
     for (nx, ny, nz, dx, dz, b, seed, dt) in EVENTS:
         e = event_e(tab, nx, ny, nz, dx, dz, b, seed)
@@ -51,10 +54,10 @@ def test_event_alone_and_in_the_mix_agree(flux):
     for (slot, e), (nx, ny, nz, dx, dz, b, seed, dt) in zip(inputs, EVENTS):
         info = mixed.info(slot)
         assert info.steps == 7 and abs(info.t - (0.4 + 7 * dt)) < 1e-12
-        alone = vah.Batch(table=tab, flux=flux)
+        alone = vah.Batch(table=tab, flux=flux, precision=precision)
         s1 = alone.add(nx, ny, nz, dx, dx, dz, 0.4, dt, 0.16, e)
         alone.step(7)
-        ev = vah.Event(nx, ny, nz, dx, dx, dz, 0.16, table=tab, t0=0.4, flux=flux)
+        ev = vah.Event(nx, ny, nz, dx, dx, dz, 0.16, table=tab, t0=0.4, flux=flux, precision=precision)
         ev.init_from_e(0.4, e)
         ev.run(0.4, dt, 7)
         ev.sync()
@@ -64,7 +67,7 @@ def test_event_alone_and_in_the_mix_agree(flux):
             np.testing.assert_array_equal(got, alone.get_field(s1, fid, False), err_msg=f"slot {slot} field {fid}")
             # pi components that vanish analytically in 2+1D carry roundoff only: floor at the e scale
             floor = 1e-3 * escale if 5 <= fid <= 15 else 0.0
-            assert rel(got, ev.get_field(fid, False), floor) < 1e-12, (slot, fid)
+            assert rel(got, ev.get_field(fid, False), floor) < (1e-5 if precision else 1e-12), (slot, fid)
         ev.close()
         alone.close()
     mixed.close()

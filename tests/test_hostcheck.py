@@ -151,3 +151,34 @@ def test_regulator_largest_ratio_path_equals_the_nine_divisions():
         L.hc_regulate(t, e, p, a.ctypes.data_as(V.P), u.ctypes.data_as(V.P), 0)
         L.hc_regulate(t, e, p, b.ctypes.data_as(V.P), u.ctypes.data_as(V.P), 1)
         assert np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+@pytest.mark.parametrize("physics,eos,shape", [("pimunu_pi", "table", (21, 19, 11)), ("pimunu", "conformal", (37, 35, 1)),
+                                               ("ideal", "table", (13, 9, 6))])
+def test_fp32_form_host_build_tracks_the_fp64_shared_face_form(physics, eos, shape):
+    """The FP32 form (vah_tile_cell.cuh: state and arithmetic in FP32, Newton
+    inversions and the closure fits in FP64, each face once with the left
+    cell's guess) compiled for the host, against the FP64 shared-face form
+    (vah_stage.cuh) on the same state: two steps within 2e-5 on e, P_L, u^mu and
+    T^{tau mu}, 1e-4 on the (randomly seeded) pi and Pi fields -- FP32 rounding;
+    any difference in the scheme would be O(1)."""
+    tab = V.eos_table() if eos == "table" else None
+    g = V.Grid(*shape, 0.2, 0.2, 0.2, 0.16, physics=physics, eos=eos,
+               zeta="crossover" if eos == "table" else "reference", table=tab)
+    f = V.smooth_initial_state(g, 0.5, amp=60.0, floor=0.5, flow=0.3, pi_amp=0.3)
+    o = V.Oracle(g)
+    V.load_state(o, f)
+    o.set_conserved(0.5, 1)
+    o.set_ghost_cells()
+    state = {fid: o.field(fid).copy() for fid in V.state_ids(g.physics)}
+    h64 = V.HostCheck(g, split=2)
+    V.load_state(h64, state)
+    t32 = V.TileCheck(g)
+    t32.load(state)
+    for n in range(2):
+        h64.step(0.5 + 0.01 * n, 0.01)
+        t32.step(0.5 + 0.01 * n, 0.01)
+    for fid in [V.E, V.PL, V.UT, V.UX, V.UY, V.UN] + list(range(V.NQ[g.physics])):
+        a, b = g.interior(t32.field(fid).astype(np.float64)), g.interior(h64.field(fid))
+        scale = max(np.max(np.abs(b)), 1e-6 * np.max(np.abs(g.interior(h64.field(V.E)))))
+        assert np.max(np.abs(a - b)) / scale < (1e-4 if 5 <= fid < 16 else 2e-5), fid

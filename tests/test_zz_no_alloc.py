@@ -126,11 +126,14 @@ def test_noalloc_stage_matches_event_step_and_oracle_twice(case):
         o.step(t, dt)
         pairs = [(fid, q[fid]) for fid in range(nq)] + [(V.E, e), (V.PP, p)] + [(V.UT + m, u[m]) for m in range(4)]
         worst = 0.0
+        escale = np.max(np.abs(g.interior(o.field(V.E))))
         for fid, arr in pairs:
             got = g.interior(arr.cpu().numpy())
+            # pi components that vanish analytically near boost invariance: floor at their natural scale
+            floor = 1e-3 * escale if 5 <= fid <= 15 else 1e-12
             if tol_event is not None:
-                assert rel_diff(got, g.interior(ev.get_field(fid))) < tol_event, (case, step, fid)
-            err = rel_diff(got, g.interior(o.field(fid)))
+                assert rel_diff(got, g.interior(ev.get_field(fid)), floor) < tol_event, (case, step, fid)
+            err = rel_diff(got, g.interior(o.field(fid)), floor)
             worst = max(worst, err)
             assert err < tol_oracle, (case, step, fid, err)
         print(f"{case} step {step}: largest normwise difference to the oracle {worst:.2e}")

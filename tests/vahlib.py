@@ -283,6 +283,51 @@ def hostcheck_lib():
     return _hc
 
 
+class TileCheck:
+    """Host build of the FP32 form (the tile kernel's face and cell arithmetic,
+    gpu-vah_b200/csrc/vah_tile_cell.cuh): float state in the reference layout."""
+
+    def __init__(self, g: Grid):
+        self.g = g
+        self.L = hostcheck_lib()
+        L = self.L
+        if not getattr(L, "_tc_ready", False):
+            L.tc_create.restype = C.c_void_p
+            L.tc_create.argtypes = [I, I, I, D, D, D, D, I, I, I, P]
+            L.tc_destroy.argtypes = [C.c_void_p]
+            L.tc_field.restype = C.POINTER(C.c_float)
+            L.tc_field.argtypes = [C.c_void_p, I]
+            L.tc_step.argtypes = [C.c_void_p, D, D]
+            L.tc_counters.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
+            L._tc_ready = True
+        tab = g.table.ctypes.data_as(P) if g.table is not None else None
+        self.h = L.tc_create(g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, g.etabar, g.physics, g.eos, g.zeta, tab)
+
+    def __del__(self):
+        try:
+            self.L.tc_destroy(self.h)
+        except Exception:
+            pass
+
+    def field(self, fid):
+        p = self.L.tc_field(self.h, fid)
+        return np.ctypeslib.as_array(p, (self.g.ncell,)) if p else None
+
+    def load(self, fields):
+        for fid, arr in fields.items():
+            dst = self.field(fid)
+            if dst is not None:
+                dst[:] = np.asarray(arr, dtype=np.float32)
+
+    def step(self, t, dt):
+        self.L.tc_step(self.h, t, dt)
+
+    def counters(self):
+        out = (C.c_ulonglong * 3)()
+        self.L.tc_counters(self.h, out)
+        return list(out)
+
+
 class HostCheck:
     def __init__(self, g: Grid, libm_exceptions=True, split=0):
         """libm_exceptions: reproduce the host libm's powf rounding in the
