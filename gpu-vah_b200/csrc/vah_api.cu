@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "vah.h"
+#include "vah_ic_device.cuh"
 #include "vah_kernels.cuh"
 #include "vah_powf_exc.h"
 #include "vah_tile.cuh"
@@ -65,6 +66,7 @@ struct vah_event {
     // FP32 form (tile layout)
     bool tile;
     void *qblock[2];                  // q and qS: nq fields each, ncell floats apart
+    void *pblock;                     // e, p of both buffers, then u, up, uS: 16 fields, ncell floats apart
     vah::TileSlot h_tslot;            // the event's tile descriptor (host copy) ...
     vah::TileSlot *d_tslot;           // ... and on the device
     vah::TileItem *d_titems;
@@ -106,6 +108,7 @@ void free_all(vah_event *ev) {
     if (ev->tile) {
         cudaFree(ev->qblock[0]);
         cudaFree(ev->qblock[1]);
+        cudaFree(ev->pblock);
         cudaFree(ev->d_tslot);
         cudaFree(ev->d_titems);
         cudaFree(ev->d_tcount);  // d_terr lives in the same allocation
@@ -115,12 +118,14 @@ void free_all(vah_event *ev) {
             cudaFree(ev->qS[n]);
         }
     }
-    for (int b = 0; b < 2; ++b)
-        for (int m = 0; m < 2; ++m) cudaFree(ev->ep[b][m]);
-    for (int m = 0; m < 4; ++m) {
-        cudaFree(ev->u[m]);
-        cudaFree(ev->up[m]);
-        cudaFree(ev->uS[m]);
+    if (!ev->tile) {
+        for (int b = 0; b < 2; ++b)
+            for (int m = 0; m < 2; ++m) cudaFree(ev->ep[b][m]);
+        for (int m = 0; m < 4; ++m) {
+            cudaFree(ev->u[m]);
+            cudaFree(ev->up[m]);
+            cudaFree(ev->uS[m]);
+        }
     }
     for (int d = 0; d < 3; ++d)
         for (int n = 0; n < 16; ++n) {
@@ -245,6 +250,17 @@ int tile_setup(vah_event *ev) {
         d.uA[m] = (float *)ev->u[m];
         d.uB[m] = (float *)ev->up[m];
         d.uS[m] = (float *)ev->uS[m];
+    }
+    const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz;
+    const long long fs = (long long)ev->ncell;
+    for (int b = 0; b < 2; ++b) {
+        const int rc = vah::tile_encode_p(&d.tmEP[b], d.ep[b][0], nx, ny, nz, ev->ncx, fs, 2);
+        if (rc != VAH_OK) return rc;
+    }
+    float *const *us[3] = {d.uA, d.uB, d.uS};
+    for (int b = 0; b < 3; ++b) {
+        const int rc = vah::tile_encode_p(&d.tmU[b], us[b][0], nx, ny, nz, ev->ncx, fs, 4);
+        if (rc != VAH_OK) return rc;
     }
     d.fstride = (long long)ev->ncell;
     d.nx = ev->lat.nx;
@@ -426,6 +442,7 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->split = vah::default_split_config();
     ev->nexc = 0;
     ev->qblock[0] = ev->qblock[1] = nullptr;
+    ev->pblock = nullptr;
     ev->d_tslot = nullptr;
     ev->d_titems = nullptr;
     ev->d_tcount = ev->d_terr = nullptr;
@@ -462,12 +479,30 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
                 alloc(&ev->qS[n]);
             }
     }
-    for (int b = 0; b < 2; ++b)
-        for (int m = 0; m < 2; ++m) alloc(&ev->ep[b][m]);
-    for (int m = 0; m < 4; ++m) {
-        alloc(&ev->u[m]);
-        alloc(&ev->up[m]);
-        alloc(&ev->uS[m]);
+    if (ev->tile) {  // the primitives as one block: (e, p) pairs and u quads are TMA boxes
+        if (rc == VAH_OK) {
+            cudaError_t e = cudaMalloc(&ev->pblock, 16 * ev->ncell * sizeof(float));
+            if (e == cudaSuccess) e = cudaMemset(ev->pblock, 0, 16 * ev->ncell * sizeof(float));
+            if (e != cudaSuccess) rc = cuda_status(e);
+        }
+        if (rc == VAH_OK) {
+            float *pb = (float *)ev->pblock;
+            for (int b = 0; b < 2; ++b)
+                for (int m = 0; m < 2; ++m) ev->ep[b][m] = pb + (2 * b + m) * ev->ncell;
+            for (int m = 0; m < 4; ++m) {
+                ev->u[m] = pb + (4 + m) * ev->ncell;
+                ev->up[m] = pb + (8 + m) * ev->ncell;
+                ev->uS[m] = pb + (12 + m) * ev->ncell;
+            }
+        }
+    } else {
+        for (int b = 0; b < 2; ++b)
+            for (int m = 0; m < 2; ++m) alloc(&ev->ep[b][m]);
+        for (int m = 0; m < 4; ++m) {
+            alloc(&ev->u[m]);
+            alloc(&ev->up[m]);
+            alloc(&ev->uS[m]);
+        }
     }
     if (opt->flux != VAH_FLUX_PER_CELL_FUSED && !ev->tile)
         for (int d = 0; d < (lat->nz > 1 ? 3 : 2); ++d)
@@ -633,6 +668,65 @@ extern "C" int vah_event_init_from_e(vah_event *ev, double t0, const double *e_i
     rc = vah_event_set_conserved(ev, t0, pl_mode == VAH_PL_ISOTROPIC);
     if (rc != VAH_OK) return rc;
     return vah_event_set_ghost_cells(ev);
+}
+
+namespace {
+
+// The e interior generated on the device (MC-Glauber when g is given, else
+// the optical Glauber profile o), then the vah_event_init_from_e sequence.
+int init_device_ic(vah_event *ev, double t0, const vah_glauber *g, const vah_optical *o, int pl_mode) {
+    if (!ev || (pl_mode != VAH_PL_REFERENCE && pl_mode != VAH_PL_ISOTROPIC)) return VAH_ERR_ARG;
+    const vah_lattice &lat = ev->lat;
+    const int A = g ? g->A : o->A;
+    const double eta_flat = g ? g->eta_flat : o->eta_flat, sigma_eta = g ? g->sigma_eta : o->sigma_eta;
+    if (A < 1 || (lat.nz > 1 && !(sigma_eta > 0))) return VAH_ERR_ARG;
+    if (g && (A > 256 || !(g->width > 0))) return VAH_ERR_ARG;
+    if (o && !(o->sigma_nn_fm2 > 0)) return VAH_ERR_ARG;
+    VAH_TRY(cudaSetDevice(ev->opt.device));
+    const size_t nxy = (size_t)lat.nx * lat.ny;
+    const size_t aux = g ? 4 * (size_t)A : (size_t)vah::kThicknessPoints + 1;
+    char *scratch = nullptr;
+    VAH_TRY(cudaMallocAsync((void **)&scratch, 256 + sizeof(double) * (aux + nxy), ev->stream));
+    unsigned long long *maxbits = (unsigned long long *)scratch;
+    double *d_aux = (double *)(scratch + 256), *d_v = d_aux + aux;
+    cudaError_t err = cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), ev->stream);
+    if (err == cudaSuccess && g) {
+        int *d_np = (int *)(scratch + 64);
+        err = vah::ic_participants_device(g->b, g->sigma_nn_fm2, A, g->ws_R, g->ws_a, g->seed, d_aux, d_np, ev->stream);
+        if (err == cudaSuccess)
+            err = vah::ic_deposit_device(d_aux, d_np, g->width, lat.nx, lat.ny, lat.dx, lat.dy, d_v, maxbits,
+                                         ev->stream);
+    } else if (err == cudaSuccess) {
+        err = vah::ic_optical_device(lat.nx, lat.ny, lat.dx, lat.dy, o->b, o->sigma_nn_fm2, A, o->ws_R, o->ws_a,
+                                     o->x_coll, d_aux, d_v, maxbits, ev->stream);
+    }
+    const double e_peak = g ? g->e_peak : o->e_peak, e_floor = g ? g->e_floor : o->e_floor;
+    if (err == cudaSuccess)
+        err = ev->elem == sizeof(float)
+                  ? vah::ic_fill_device<float>(d_v, maxbits, lat.nx, lat.ny, lat.nz, ev->ncx, lat.dz, eta_flat,
+                                               sigma_eta, e_peak, e_floor, (float *)ev->ep[ev->cur][0], ev->stream)
+                  : vah::ic_fill_device<double>(d_v, maxbits, lat.nx, lat.ny, lat.nz, ev->ncx, lat.dz, eta_flat,
+                                                sigma_eta, e_peak, e_floor, (double *)ev->ep[ev->cur][0], ev->stream);
+    const cudaError_t ferr = cudaFreeAsync(scratch, ev->stream);
+    VAH_TRY(err);
+    VAH_TRY(ferr);
+    int rc = ev->elem == sizeof(float) ? init_primitives_t<float>(ev) : init_primitives_t<double>(ev);
+    if (rc != VAH_OK) return rc;
+    rc = vah_event_set_conserved(ev, t0, pl_mode == VAH_PL_ISOTROPIC);
+    if (rc != VAH_OK) return rc;
+    return vah_event_set_ghost_cells(ev);
+}
+
+}  // namespace
+
+extern "C" int vah_event_init_glauber(vah_event *ev, double t0, const vah_glauber *g, int pl_mode) {
+    if (!g) return VAH_ERR_ARG;
+    return init_device_ic(ev, t0, g, nullptr, pl_mode);
+}
+
+extern "C" int vah_event_init_optical_glauber(vah_event *ev, double t0, const vah_optical *o, int pl_mode) {
+    if (!o) return VAH_ERR_ARG;
+    return init_device_ic(ev, t0, nullptr, o, pl_mode);
 }
 
 extern "C" int vah_event_set_ghost_cells(vah_event *ev) {

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "vah.h"
+#include "vah_ic_device.cuh"
 #include "vah_kernels.cuh"
 #include "vah_powf_exc.h"
 #include "vah_tile.cuh"
@@ -192,42 +193,6 @@ __global__ void hot_init_kernel(const S *e, unsigned char *hot, double e_freeze,
         const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
         const long long s = (i + 2) + (long long)pitch * ((j + 2) + (long long)(ny + 4) * (k + 2));
         hot[s] = (double)e[s] > e_freeze;
-    }
-}
-
-// MC-Glauber deposit on the device: v(x, y) = sum over participants of
-// exp(-r^2 / (2 w^2)) (cut at r = 8 w, as the host generator), one thread per
-// transverse cell; the maximum goes to maxbits (positive doubles order like
-// their bit patterns).
-__global__ void glauber_deposit_kernel(const double *__restrict__ pxy, int np, double inv2w2, double cut2, int nx,
-                                       int ny, double dx, double dy, double *vxy, unsigned long long *maxbits) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nx * ny; c += gridDim.x * blockDim.x) {
-        const int i = c % nx, j = c / nx;
-        const double x = (i - (nx - 1) / 2.) * dx, y = (j - (ny - 1) / 2.) * dy;
-        double v = 0;
-        for (int p = 0; p < np; ++p) {
-            const double rx = x - pxy[2 * p], ry = y - pxy[2 * p + 1];
-            const double r2 = rx * rx + ry * ry;
-            if (r2 < cut2) v += exp(-r2 * inv2w2);
-        }
-        vxy[c] = v;
-        atomicMax(maxbits, (unsigned long long)__double_as_longlong(v));
-    }
-}
-
-// e(x, y, eta) = e_peak v / max v * f(eta) + e_floor into the slot's interior
-// (a flat floor when no nucleon collided).
-template <typename S>
-__global__ void glauber_fill_kernel(const double *__restrict__ vxy, const unsigned long long *__restrict__ maxbits,
-                                    const double *__restrict__ feta, int nx, int ny, int nz, int pitch,
-                                    double e_peak, double e_floor, S *e) {
-    const double vmax = __longlong_as_double((long long)*maxbits);
-    const long long n = (long long)nx * ny * nz;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        const long long t = c % ((long long)nx * ny);
-        const int k = (int)(c / ((long long)nx * ny)), i = (int)(t % nx), j = (int)(t / nx);
-        const double exy = vmax > 0 ? e_peak * vxy[t] / vmax : 0.0;
-        e[(i + 2) + (long long)pitch * ((j + 2) + (long long)(ny + 4) * (k + 2))] = (S)(exy * feta[k] + e_floor);
     }
 }
 
@@ -555,6 +520,18 @@ int fill_slot(vah_batch *b, int slot) {
             t.uB[m] = (float *)d.uB[m];
             t.uS[m] = (float *)d.uS[m];
         }
+        // the slot's arrays follow one another `per` bytes apart: (e, p) pairs and u quads are blocks
+        for (int bb = 0; bb < 2; ++bb) {
+            const int rc = vah::tile_encode_p(&t.tmEP[bb], t.ep[bb][0], sl.lat.nx, sl.lat.ny, sl.lat.nz, d.ncx,
+                                              t.fstride, 2);
+            if (rc != VAH_OK) return rc;
+        }
+        float *const *us[3] = {t.uA, t.uB, t.uS};
+        for (int bb = 0; bb < 3; ++bb) {
+            const int rc = vah::tile_encode_p(&t.tmU[bb], us[bb][0], sl.lat.nx, sl.lat.ny, sl.lat.nz, d.ncx,
+                                              t.fstride, 4);
+            if (rc != VAH_OK) return rc;
+        }
         t.nx = d.nx;
         t.ny = d.ny;
         t.nz = d.nz;
@@ -738,34 +715,23 @@ vah::FieldSet<S> fs(S *const *p, int n) {
 }
 
 // Device-generated initial energy density (vah_batch_add_glauber) into the
-// slot's e interior; scratch from the batch's pool, freed in stream order.
+// slot's e interior: participants sampled, deposited and normalised on the
+// GPU; scratch from the batch's pool, freed in stream order.
 template <typename S>
 int glauber_slot(vah_batch *b, const SlotDesc<S> &d, const vah_lattice &lat, const vah_glauber &g) {
-    std::vector<double> pxy(2 * (size_t)(2 * g.A));
-    int np = 0;
-    int rc = vah_ic_mc_glauber_participants(g.b, g.sigma_nn_fm2, g.A, g.ws_R, g.ws_a, g.seed, pxy.data(), 2 * g.A, &np);
-    if (rc != VAH_OK) return rc;
-    std::vector<double> feta(lat.nz, 1.0);
-    if (lat.nz > 1 && (rc = vah_ic_longitudinal(lat.nz, lat.dz, g.eta_flat, g.sigma_eta, feta.data())) != VAH_OK)
-        return rc;
+    if (g.A < 1 || g.A > 256 || !(g.width > 0) || (lat.nz > 1 && !(g.sigma_eta > 0))) return VAH_ERR_ARG;
     const size_t nxy = (size_t)lat.nx * lat.ny;
-    const size_t bytes = 256 + sizeof(double) * (2 * (size_t)std::max(np, 1) + nxy + lat.nz);
+    const size_t bytes = 256 + sizeof(double) * (4 * (size_t)g.A + nxy);
     char *scratch = nullptr;
     VAH_TRY(cudaMallocFromPoolAsync((void **)&scratch, bytes, b->pool, b->stream));
     unsigned long long *maxbits = (unsigned long long *)scratch;
-    double *d_pxy = (double *)(scratch + 256), *d_v = d_pxy + 2 * (size_t)std::max(np, 1), *d_f = d_v + nxy;
+    int *d_np = (int *)(scratch + 64);
+    double *d_pxy = (double *)(scratch + 256), *d_v = d_pxy + 4 * (size_t)g.A;
     VAH_TRY(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), b->stream));
-    if (np) VAH_TRY(cudaMemcpyAsync(d_pxy, pxy.data(), sizeof(double) * 2 * np, cudaMemcpyHostToDevice, b->stream));
-    VAH_TRY(cudaMemcpyAsync(d_f, feta.data(), sizeof(double) * lat.nz, cudaMemcpyHostToDevice, b->stream));
-    const int block = 128;
-    vah::glauber_deposit_kernel<<<(int)std::min<size_t>((nxy + block - 1) / block, 148 * 16), block, 0, b->stream>>>(
-        d_pxy, np, 1.0 / (2 * g.width * g.width), 64 * g.width * g.width, lat.nx, lat.ny, lat.dx, lat.dy, d_v,
-        maxbits);
-    VAH_TRY(cudaGetLastError());
-    vah::glauber_fill_kernel<S><<<(int)std::min<size_t>((nxy * lat.nz + block - 1) / block, 148 * 16), block, 0,
-                                  b->stream>>>(d_v, maxbits, d_f, lat.nx, lat.ny, lat.nz, d.ncx, g.e_peak,
-                                               g.e_floor, d.ep[0][0]);
-    VAH_TRY(cudaGetLastError());
+    VAH_TRY(vah::ic_participants_device(g.b, g.sigma_nn_fm2, g.A, g.ws_R, g.ws_a, g.seed, d_pxy, d_np, b->stream));
+    VAH_TRY(vah::ic_deposit_device(d_pxy, d_np, g.width, lat.nx, lat.ny, lat.dx, lat.dy, d_v, maxbits, b->stream));
+    VAH_TRY(vah::ic_fill_device<S>(d_v, maxbits, lat.nx, lat.ny, lat.nz, d.ncx, lat.dz, g.eta_flat, g.sigma_eta,
+                                   g.e_peak, g.e_floor, d.ep[0][0], b->stream));
     VAH_TRY(cudaFreeAsync(scratch, b->stream));
     return VAH_OK;
 }

@@ -85,6 +85,32 @@ int tile_encode_q(CUtensorMap *tm, const float *base, int nx, int ny, int nz, in
     return r == CUDA_SUCCESS ? VAH_OK : VAH_ERR_CUDA;
 }
 
+int tile_encode_p(CUtensorMap *tm, const float *base, int nx, int ny, int nz, int pitch, long long fstride, int nf) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return VAH_ERR_NODEVICE;
+    const bool is3d = nz > 1;
+    const int ncy = ny + 4, ncz = nz + 4;
+    if (pitch % 4 || fstride % 4 || ((uintptr_t)base & 15)) return VAH_ERR_ARG;
+    const cuuint64_t dims[4] = {(cuuint64_t)(nx + 4), (cuuint64_t)ncy, (cuuint64_t)ncz, (cuuint64_t)nf};
+    const cuuint64_t strides[3] = {(cuuint64_t)pitch * 4, (cuuint64_t)pitch * ncy * 4, (cuuint64_t)fstride * 4};
+    cuuint32_t box[4];
+    if (is3d) {
+        box[0] = TileShape<true>::PBX;
+        box[1] = TileShape<true>::PBY;
+        box[2] = TileShape<true>::PBZ;
+    } else {
+        box[0] = TileShape<false>::PBX;
+        box[1] = TileShape<false>::PBY;
+        box[2] = TileShape<false>::PBZ;
+    }
+    box[3] = (cuuint32_t)nf;
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? VAH_OK : VAH_ERR_CUDA;
+}
+
 void tile_items(std::vector<TileItem> &out, int slot, int nx, int ny, int nz) {
     const bool is3d = nz > 1;
     const int tx = is3d ? TileShape<true>::TX : TileShape<false>::TX;

@@ -40,11 +40,16 @@ constexpr int kTileThreads = 256;
 template <bool IS3D>
 struct TileShape {
     static constexpr int TX = IS3D ? 8 : 16, TY = IS3D ? 8 : 16, TZ = IS3D ? 4 : 1;
-    static constexpr int BX = TX + 4, BY = TY + 4, BZ = IS3D ? TZ + 4 : 1;  // TMA box (halo 2; 2+1D: one plane)
-    static constexpr int BOXN = BX * BY * BZ;                               // cells of the box
+    // box of the conserved fields: halo 2 (2+1D: the one plane)
+    static constexpr int BX = TX + 4, BY = TY + 4, BZ = IS3D ? TZ + 4 : 1;
+    static constexpr int BOXN = BX * BY * BZ;
+    // box of the primitives e, p, u: halo 1 in y and z; x as the conserved box (a 16-byte aligned start)
+    static constexpr int PBX = BX, PBY = TY + 2, PBZ = IS3D ? TZ + 2 : 1;
+    static constexpr int PBOXN = PBX * PBY * PBZ;
     static constexpr int NBX = TY * TZ, NBY = TX * TZ, NBZ = IS3D ? TX * TY : 0;  // lower boundary faces per axis
-    static constexpr int NB = NBX + NBY + NBZ;
+    static constexpr int NBXY = NBX + NBY;
     static_assert(TX * TY * TZ == kTileThreads, "one thread per cell");
+    static_assert(NBXY <= kTileThreads && NBZ <= NBXY, "boundary faces: one per thread, z reusing the x/y buffer");
     static_assert((BX * 4) % 16 == 0, "TMA box rows must be a multiple of 16 bytes");
 };
 
@@ -57,7 +62,9 @@ struct TileShape {
 // parity flips); uS = stage 1's u. Cell (i, j, k) of the ghosted grid is at
 // i + pitch (j + ncy k), pitch a multiple of 4 floats.
 struct alignas(64) TileSlot {
-    CUtensorMap tmQ[2];  // over Q[0], Q[1]
+    CUtensorMap tmQ[2];   // over Q[0], Q[1] (N_q fields)
+    CUtensorMap tmEP[2];  // over ep[0], ep[1] (e, p: two fields, fstride apart)
+    CUtensorMap tmU[3];   // over uA, uB, uS (four fields each, fstride apart)
     float *Q[2];
     float *ep[2][2];
     float *uA[4], *uB[4], *uS[4];
@@ -152,18 +159,24 @@ __device__ __forceinline__ void tile_count(unsigned long long *c, unsigned v) {
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(c, (unsigned long long)s);
 }
 
-// The dynamic shared memory of one block: TMA box, y/z face buffer, lower
-// boundary faces, and (after them) the mbarrier and the tile index.
+// The dynamic shared memory of one block: the TMA boxes (conserved fields,
+// then e, p, u), the face buffer of the +1/2 faces along y, then z, the lower
+// boundary faces (x and y, then z), and the mbarrier and the tile index.
 template <int PHYS, bool IS3D>
 struct TileSmem {
     using SH = TileShape<IS3D>;
     static constexpr int NQ = Phys<PHYS>::NQ;
-    static constexpr size_t box_floats = (size_t)SH::BOXN * NQ;
+    static constexpr size_t pad32(size_t n) { return (n + 31) / 32 * 32; }  // to 128-byte multiples
+    // each TMA destination starts on a 128-byte boundary
+    static constexpr size_t box_floats = pad32((size_t)SH::BOXN * NQ);
+    static constexpr size_t ep_floats = pad32((size_t)SH::PBOXN * 2);
+    static constexpr size_t u_floats = pad32((size_t)SH::PBOXN * 4);
     static constexpr size_t face_floats = (size_t)kTileThreads * NQ;
-    static constexpr size_t bnd_floats = (size_t)SH::NB * NQ;
-    static constexpr size_t box_bytes = box_floats * 4;
-    // the mbarrier (8 bytes) and the tile index (4 bytes) follow the floats
-    static constexpr size_t bar_offset = ((box_floats + face_floats + bnd_floats) * 4 + 15) / 16 * 16;
+    static constexpr size_t bnd_floats = (size_t)SH::NBXY * NQ;
+    static constexpr size_t box_bytes = (size_t)SH::BOXN * NQ * 4, ep_bytes = (size_t)SH::PBOXN * 2 * 4,
+                            u_bytes = (size_t)SH::PBOXN * 4 * 4;  // what the copies write
+    static constexpr size_t bar_offset =
+        ((box_floats + ep_floats + u_floats + face_floats + bnd_floats) * 4 + 15) / 16 * 16;
     static constexpr size_t bytes = bar_offset + 16;
 };
 
@@ -176,16 +189,21 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     using SM = TileSmem<PHYS, IS3D>;
     constexpr int NQ = Phys<PHYS>::NQ;
     constexpr int TX = SH::TX, TY = SH::TY, BX = SH::BX, BY = SH::BY, BOXN = SH::BOXN;
+    constexpr int PBX = SH::PBX, PBY = SH::PBY, PBOXN = SH::PBOXN;
+    constexpr int SY = BX, SZ = BX * BY, PSY = PBX, PSZ = PBX * PBY;
     extern __shared__ __align__(1024) float tile_smem[];
     float *sQ = tile_smem;                     // [NQ][BZ][BY][BX]
-    float *sF = sQ + SM::box_floats;           // [NQ][256]: +1/2 faces along y, then z
-    float *sB = sF + SM::face_floats;          // [NQ][NB]: lower boundary faces (x, y, z)
+    float *sP = sQ + SM::box_floats;           // [2][PBZ][PBY][PBX]: e, p
+    float *sU = sP + SM::ep_floats;            // [4][PBZ][PBY][PBX]: ut, ux, uy, un
+    float *sF = sU + SM::u_floats;             // [NQ][256]: +1/2 faces along y, then z
+    float *sB = sF + SM::face_floats;          // [NQ][NBXY]: lower boundary faces (x, y; then z)
     unsigned long long *bar = (unsigned long long *)((char *)tile_smem + SM::bar_offset);
     int &s_item = *(int *)(bar + 1);
+    const float *const sE = sP, *const sPp = sP + PBOXN, *const sUX = sU + PBOXN, *const sUY = sU + 2 * PBOXN;
 
     const int tid = threadIdx.x;
     const int lx = tid % TX, ly = (tid / TX) % TY, lz = tid / (TX * TY);
-    if (smem_u32(sQ) & 127u) {  // the TMA destination must be 128-byte aligned: report, issue nothing
+    if (smem_u32(sQ) & 127u) {  // the TMA destinations must be 128-byte aligned: report, issue nothing
         if (tid == 0) atomicOr(err, kTileErrAlign);
         return;
     }
@@ -209,23 +227,22 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         float *const *u_p = c.parity ? d.uA : d.uB;      // u^{n-1}
         // stage inputs and outputs (FullyDiscreteKurganovTadmorScheme.cpp:761-789)
         float *Qout = d.Q[stage == 1 ? 1 : 0];
-        const float *Ein = d.ep[stage == 1 ? 0 : 1][0], *Pin_p = d.ep[stage == 1 ? 0 : 1][1];
         float *Eout = d.ep[stage == 1 ? 1 : 0][0], *Pout_p = d.ep[stage == 1 ? 1 : 0][1];
-        float *const *Uin = stage == 1 ? u_n : d.uS;
         float *const *Uup = stage == 1 ? u_p : u_n;  // previous-stage u (d_tau u)
-        float *const *Ugs = u_n;                     // the cell inversion's Newton guess
         float *const *Uout = stage == 1 ? d.uS : u_p;
-        const float *UX = Uin[1], *UY = Uin[2];
         const long long fs = d.fstride;
         const int pitch = d.pitch;
         const long long plane = (long long)pitch * d.ncy;
         const double t_src = stage == 1 ? c.t : c.t + dt;
         const double t_inv = c.t + dt;
 
-        if (tid == 0) {
-            fence_proxy_async_smem();  // the previous tile's generic reads of sQ come first
-            mbar_expect_tx(bar, (unsigned)SM::box_bytes);
-            tma_load_4d(sQ, &d.tmQ[stage == 1 ? 0 : 1], bar, it.i0, it.j0, IS3D ? it.k0 : 2, 0);
+        if (tid == 0) {  // the stage inputs: conserved fields (halo 2), e and p, u (halo 1)
+            fence_proxy_async_smem();  // the previous tile's generic reads of these buffers come first
+            mbar_expect_tx(bar, (unsigned)(SM::box_bytes + SM::ep_bytes + SM::u_bytes));
+            const int z0 = IS3D ? it.k0 : 2, pz0 = IS3D ? it.k0 + 1 : 2;
+            tma_load_4d(sQ, &d.tmQ[stage == 1 ? 0 : 1], bar, it.i0, it.j0, z0, 0);
+            tma_load_4d(sP, &d.tmEP[stage == 1 ? 0 : 1], bar, it.i0, it.j0 + 1, pz0, 0);
+            tma_load_4d(sU, &d.tmU[stage == 1 ? c.parity : 2], bar, it.i0, it.j0 + 1, pz0, 0);
         }
         if (!mbar_wait(bar, phase, 1u << 22)) {
             if (tid == 0) atomicOr(err, kTileErrTimeout);
@@ -235,76 +252,51 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         }
         phase ^= 1u;
 
-        // this thread's cell, in interior and ghosted coordinates
+        // this thread's cell, in interior and ghosted coordinates, and in the boxes
         const int ci = it.i0 + lx, cj = it.j0 + ly, ck = it.k0 + lz;
         const bool live = ci < d.nx && cj < d.ny && ck < d.nz;
-        const int gi = ci + 2, gj = cj + 2, gk = ck + 2;
-        const long long s = gi + (long long)pitch * gj + plane * gk;
-        const int bc = (lx + 2) + BX * ((ly + 2) + BY * (IS3D ? lz + 2 : 0));  // box index of the cell
-        constexpr int SY = BX, SZ = BX * BY;
-
-        // ---- faces ----
+        const long long s = (ci + 2) + (long long)pitch * (cj + 2) + plane * (ck + 2);
+        const int bc = (lx + 2) + BX * ((ly + 2) + BY * (IS3D ? lz + 2 : 0));
+        const int pc = (lx + 2) + PBX * ((ly + 1) + PBY * (IS3D ? lz + 1 : 0));
         const BoxQ<BOXN> bq{sQ};
         unsigned ffail = 0, fnan = 0;
-        float Hx[NQ];
+        auto count = [&](unsigned f) {
+            ffail += f & 255u;
+            fnan |= f >> 8;
+        };
         // Newton guess and fallback energy of the faces whose left cell is this one
-        double e0 = 0.0, uT0 = 0.0;
-        if (live) {
-            const double ux = (double)UX[s], uy = (double)UY[s];
-            e0 = (double)Ein[s];
-            uT0 = sqrt(fabs(ux * ux + uy * uy));
-        }
-        {   // +1/2 along x of this cell
-            if (live) {
-                const unsigned f = tile_face<PHYS>(bq, bc, 1, 0, t_src, e0, uT0, Hx);
-                ffail += f & 255u;
-                fnan |= f >> 8;
-            } else {
+        const double e0 = (double)sE[pc], ux0 = (double)sUX[pc], uy0 = (double)sUY[pc];
+        const double uT0 = sqrt(fabs(ux0 * ux0 + uy0 * uy0));
+
+        // ---- faces: +1/2 along x (registers), the x and y lower boundary faces, +1/2 along y ----
+        float Hx[NQ];
+        if (live) count(tile_face<PHYS>(bq, bc, 1, 0, t_src, e0, uT0, Hx, 1));
+        else
 #pragma unroll
-                for (int n = 0; n < NQ; ++n) Hx[n] = 0.0f;
-            }
-        }
-        if (tid < SH::NB) {  // lower boundary faces of the tile: left cell in the halo
-            int b = tid, dir, L, bi, bj, bk;
-            if (b < SH::NBX) {
-                dir = 0; bi = 1; bj = 2 + b % TY; bk = IS3D ? 2 + b / TY : 0;
-            } else if (b < SH::NBX + SH::NBY) {
-                b -= SH::NBX; dir = 1; bi = 2 + b % TX; bj = 1; bk = IS3D ? 2 + b / TX : 0;
-            } else {
-                b -= SH::NBX + SH::NBY; dir = 2; bi = 2 + b % TX; bj = 2 + b / TX; bk = 1;
-            }
-            L = bi + BX * (bj + BY * bk);
-            // the right cell (first of the tile along dir) decides whether the face is needed
+            for (int n = 0; n < NQ; ++n) Hx[n] = 0.0f;
+        // lower boundary face b of the tile along `dir`; the left cell is in the halo
+        auto boundary = [&](int b, int dir, float *dst) {
+            int bi, bj, bk;  // left cell in the conserved box
+            if (dir == 0) { bi = 1; bj = 2 + b % TY; bk = IS3D ? 2 + b / TY : 0; }
+            else if (dir == 1) { bi = 2 + b % TX; bj = 1; bk = IS3D ? 2 + b / TX : 0; }
+            else { bi = 2 + b % TX; bj = 2 + b / TX; bk = 1; }
             const int ri = it.i0 + bi - 2 + (dir == 0), rj = it.j0 + bj - 2 + (dir == 1),
-                      rk = it.k0 + (IS3D ? bk - 2 : 0) + (dir == 2);
-            float Hb[NQ];
+                      rk = it.k0 + (IS3D ? bk - 2 : 0) + (dir == 2);  // the right cell: the tile's first
             if (ri < d.nx && rj < d.ny && rk < d.nz) {
-                const long long sl = (it.i0 + bi) + (long long)pitch * (it.j0 + bj) + plane * (IS3D ? it.k0 + bk : 2);
-                const double el = (double)Ein[sl], ux = (double)UX[sl], uy = (double)UY[sl];
-                const unsigned f = tile_face<PHYS>(bq, L, dir == 0 ? 1 : (dir == 1 ? SY : SZ), dir, t_src, el,
-                                                         sqrt(fabs(ux * ux + uy * uy)), Hb);
-                ffail += f & 255u;
-                fnan |= f >> 8;
+                const int pl = bi + PBX * ((bj - 1) + PBY * (IS3D ? bk - 1 : 0));
+                const double el = (double)sE[pl], ux = (double)sUX[pl], uy = (double)sUY[pl];
+                count(tile_face<PHYS>(bq, bi + BX * (bj + BY * bk), dir == 0 ? 1 : (dir == 1 ? SY : SZ), dir, t_src, el,
+                                      sqrt(fabs(ux * ux + uy * uy)), dst, SH::NBXY));
             } else {
 #pragma unroll
-                for (int n = 0; n < NQ; ++n) Hb[n] = 0.0f;
+                for (int n = 0; n < NQ; ++n) dst[n * SH::NBXY] = 0.0f;
             }
+        };
+        if (tid < SH::NBXY) boundary(tid < SH::NBX ? tid : tid - SH::NBX, tid < SH::NBX ? 0 : 1, sB + tid);
+        if (live) count(tile_face<PHYS>(bq, bc, SY, 1, t_src, e0, uT0, sF + tid, kTileThreads));
+        else
 #pragma unroll
-            for (int n = 0; n < NQ; ++n) sB[n * SH::NB + tid] = Hb[n];
-        }
-        {   // +1/2 along y
-            float Hy[NQ];
-            if (live) {
-                const unsigned f = tile_face<PHYS>(bq, bc, SY, 1, t_src, e0, uT0, Hy);
-                ffail += f & 255u;
-                fnan |= f >> 8;
-            } else {
-#pragma unroll
-                for (int n = 0; n < NQ; ++n) Hy[n] = 0.0f;
-            }
-#pragma unroll
-            for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = Hy[n];
-        }
+            for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = 0.0f;
         __syncthreads();
 
         // flux differences: x through warp shuffles (lane - 1 holds the -1/2
@@ -314,29 +306,22 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 #pragma unroll
         for (int n = 0; n < NQ; ++n) {
             float hm = __shfl_up_sync(0xffffffffu, Hx[n], 1, TX);
-            if (lx == 0) hm = sB[n * SH::NB + (ly + TY * lz)];
-            const float ym = ly > 0 ? sF[n * kTileThreads + tid - TX] : sB[n * SH::NB + SH::NBX + lx + TX * lz];
+            if (lx == 0) hm = sB[n * SH::NBXY + (ly + TY * lz)];
+            const float ym = ly > 0 ? sF[n * kTileThreads + tid - TX] : sB[n * SH::NBXY + SH::NBX + lx + TX * lz];
             flux[n] = cx * (hm - Hx[n]) + cy * (ym - sF[n * kTileThreads + tid]);
         }
-        if (IS3D) {
-            __syncthreads();  // the y faces are consumed
-            float Hz[NQ];
-            if (live) {
-                const unsigned f = tile_face<PHYS>(bq, bc, SZ, 2, t_src, e0, uT0, Hz);
-                ffail += f & 255u;
-                fnan |= f >> 8;
-            } else {
+        if (IS3D) {  // +1/2 along z and the z lower boundary faces (reusing the buffers)
+            __syncthreads();
+            if (tid < SH::NBZ) boundary(tid, 2, sB + tid);
+            if (live) count(tile_face<PHYS>(bq, bc, SZ, 2, t_src, e0, uT0, sF + tid, kTileThreads));
+            else
 #pragma unroll
-                for (int n = 0; n < NQ; ++n) Hz[n] = 0.0f;
-            }
-#pragma unroll
-            for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = Hz[n];
+                for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = 0.0f;
             __syncthreads();
 #pragma unroll
             for (int n = 0; n < NQ; ++n) {
-                const float zm = lz > 0 ? sF[n * kTileThreads + tid - TX * TY]
-                                        : sB[n * SH::NB + SH::NBX + SH::NBY + lx + TX * ly];
-                flux[n] += cz * (zm - Hz[n]);
+                const float zm = lz > 0 ? sF[n * kTileThreads + tid - TX * TY] : sB[n * SH::NBXY + lx + TX * ly];
+                flux[n] += cz * (zm - sF[n * kTileThreads + tid]);
             }
         }
         if (d.counters) {
@@ -346,15 +331,18 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 
         // ---- the cell ----
         if (live) {
-            const long long sy = pitch, sz = plane;
             TilePrims pr;
-            pr.E = Ein;
-            pr.P = Pin_p;
+            pr.E = sE;
+            pr.P = sPp;
+#pragma unroll
             for (int m = 0; m < 4; ++m) {
-                pr.U[m] = Uin[m];
+                pr.U[m] = sU + m * PBOXN;
                 pr.UP[m] = Uup[m];
-                pr.G[m] = Ugs[m];
+                pr.G[m] = u_n[m];
             }
+            pr.pi = pc;
+            pr.psy = PSY;
+            pr.psz = PSZ;
             struct {
                 const float *q;
                 long long fs;
@@ -362,8 +350,8 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             } qavg{d.Q[0], fs};
             float val[NQ], e, p, u[4], rmap[11];
             int bad = 0;
-            const int st = tile_cell<PHYS, IS3D>(bq, bc, SY, SZ, pr, s, sy, sz, flux, qavg, stage == 2, eos, t_src,
-                                                 t_inv, dt, d.dx, d.dy, d.dz, d.etabar, val, e, p, u,
+            const int st = tile_cell<PHYS, IS3D>(bq, bc, SY, SZ, pr, s, flux, qavg, stage == 2, eos, t_src, t_inv, dt,
+                                                 d.dx, d.dy, d.dz, d.etabar, val, e, p, u,
                                                  d.regmap[0] ? rmap : nullptr, bad);
             if (d.regmap[0] && Phys<PHYS>::PIMUNU)
                 for (int m = 0; m < 11; ++m) d.regmap[m][s] = (double)rmap[m];
@@ -381,6 +369,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 }
             }
             // stores, and the face ghost layers of boundary cells (setGhostCellsKernelI/J/K)
+            const long long sy = pitch, sz = plane;
             auto store = [&](long long at) {
 #pragma unroll
                 for (int n = 0; n < NQ; ++n) Qout[n * fs + at] = val[n];
@@ -397,7 +386,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             if (ck == 0) { store(s - sz); store(s - 2 * sz); }
             if (ck == d.nz - 1) { store(s + sz); store(s + 2 * sz); }
         }
-        __syncthreads();  // every read of sQ, sF, sB of this tile is done
+        __syncthreads();  // every read of this tile's buffers is done
     }
 }
 
@@ -416,6 +405,10 @@ inline int tile_pitch(int nx) { return (nx + 4 + 3) / 4 * 4; }
 // Rank-4 tensor map (x, y, z, field) over a block of nq fields of float,
 // fstride floats apart, with the box of the tile shape. Returns a VAH_* status.
 int tile_encode_q(CUtensorMap *tm, const float *base, int nx, int ny, int nz, int pitch, long long fstride, int nq);
+
+// The same over a block of nf primitive fields (e, p or u^mu), with the box of
+// the primitives (halo 1 in y and z).
+int tile_encode_p(CUtensorMap *tm, const float *base, int nx, int ny, int nz, int pitch, long long fstride, int nf);
 
 // The tiles covering an event's interior, appended to `out`.
 void tile_items(std::vector<TileItem> &out, int slot, int nx, int ny, int nz);

@@ -6,6 +6,16 @@
 
 #include "vah_physics.cuh"
 
+// The face evaluation is called from four places per tile; kept out of line
+// on the device so that the kernel's code fits the instruction cache.
+#if defined(__CUDACC__) && !defined(VAH_TILE_FACE_INLINE)
+#define VAH_TILE_FACE __host__ __device__ __noinline__
+#elif defined(__CUDACC__)
+#define VAH_TILE_FACE __host__ __device__ __forceinline__
+#else
+#define VAH_TILE_FACE inline
+#endif
+
 namespace vah {
 
 // --------------------------------------------- the FP32 form's cell algebra --
@@ -29,11 +39,12 @@ struct ArrQ {
 // Kurganov-Tadmor flux through the face between cells L and L + st
 // (SemiDiscreteKurganovTadmorScheme.cpp:13-57, FluxLimiter.cpp:28-33): the
 // states reconstructed in FP32, inverted in FP64 from the guess uT (the left
-// cell's |u_T|), H = wR qR + wL qL in FP32. Returns the number of inversions
+// cell's |u_T|), H[n hs] = wR qR + wL qL in FP32 (hs: the stride of the
+// destination, e.g. a shared face buffer). Returns the number of inversions
 // that fell back; bit 8 flags a NaN (ePrev: the left cell's e).
 template <int PHYS, typename QA>
-VAH_HD unsigned tile_face(const QA &q, long long L, long long st, int dir, double t, double ePrev, double uT,
-                          float *H) {
+VAH_TILE_FACE unsigned tile_face(const QA q, long long L, long long st, int dir, double t, double ePrev, double uT,
+                                 float *H, int hs) {
     constexpr int NQ = Phys<PHYS>::NQ;
     float qR[NQ], qL[NQ];
 #pragma unroll
@@ -59,46 +70,51 @@ VAH_HD unsigned tile_face(const QA &q, long long L, long long st, int dir, doubl
     const double a = fmax(fabs(vL), fabs(vR));
     const float wR = (float)(0.5 * (vR - a)), wL = (float)(0.5 * (vL + a));
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) H[n] = wR * qR[n] + wL * qL[n];
+    for (int n = 0; n < NQ; ++n) H[n * hs] = wR * qR[n] + wL * qL[n];
     return (stR != 0) + (stL != 0) + ((stR == 2 || stL == 2) ? 256u : 0u);
 }
 
-// Stage-input primitives, read at the cell and its +-1 neighbours: e, p, u
-// (stencil), the previous stage's u (centre) and the inversion's guess u.
+// Stage-input primitives: e, p, u read at the cell and its +-1 neighbours
+// (index pi, strides psy, psz: the shared-memory box on the device, the
+// field arrays on the host), and at the cell only (global index s) the
+// previous stage's u and the inversion's guess u.
 struct TilePrims {
-    const float *E, *P, *U[4], *UP[4], *G[4];
+    const float *E, *P, *U[4];
+    long long pi, psy, psz;
+    const float *UP[4], *G[4];
 };
 
 // The cell part of a stage (eulerStepKernelSource, the axis sources,
 // [the convex combination], setInferredVariablesKernel, the regulator):
 // q: the stage-input conserved fields at box index b (strides bsy, bsz);
-// pr: primitives at global index s (strides sy, sz); flux[n]: the flux
+// pr: the primitives; s: the cell's global index; flux[n]: the flux
 // differences dt/h (H(-1/2) - H(+1/2)) summed over the axes; qavg(n, s): q^n
 // (stage 2). Writes the new conserved values, e, p, u; returns the inversion's
 // status (0 converged, 1 fallback, 2 NaN) and sets bad when a source is NaN.
 template <int PHYS, bool IS3D, typename QA, typename QV>
 VAH_HD int tile_cell(const QA &q, long long b, long long bsy, long long bsz, const TilePrims &pr, long long s,
-                     long long sy, long long sz, const float *flux, const QV &qavg, bool stage2, const Eos &eos,
-                     double t_src, double t_inv, double dt, double dx, double dy, double dz, double etabar,
-                     float *val, float &e, float &p, float *u, float *rmap, int &bad) {
+                     const float *flux, const QV &qavg, bool stage2, const Eos &eos, double t_src, double t_inv,
+                     double dt, double dx, double dy, double dz, double etabar, float *val, float &e, float &p,
+                     float *u, float *rmap, int &bad) {
     constexpr int NQ = Phys<PHYS>::NQ;
     float qc[NQ];
 #pragma unroll
     for (int n = 0; n < NQ; ++n) qc[n] = q(n, b);
     const float fx = (float)(0.5 / dx), fy = (float)(0.5 / dy), fz = (float)(0.5 / dz);
     const float *E = pr.E, *PP = pr.P, *UT = pr.U[0], *UX = pr.U[1], *UY = pr.U[2], *UN = pr.U[3];
+    const long long c = pr.pi, sy = pr.psy, sz = pr.psz;
     CellGradT<float> g;
-    g.e = E[s];
-    g.p = PP[s];
-    g.ut = UT[s];
-    g.ux = UX[s];
-    g.uy = UY[s];
-    g.un = UN[s];
+    g.e = E[c];
+    g.p = PP[c];
+    g.ut = UT[c];
+    g.ux = UX[c];
+    g.uy = UY[c];
+    g.un = UN[c];
     g.utp = pr.UP[0][s];
     g.uxp = pr.UP[1][s];
     g.uyp = pr.UP[2][s];
     g.unp = pr.UP[3][s];
-#define VAH_TCD(A, off, f) (((A)[s + (off)] - (A)[s - (off)]) * (f))
+#define VAH_TCD(A, off, f) (((A)[c + (off)] - (A)[c - (off)]) * (f))
     g.dxut = VAH_TCD(UT, 1, fx); g.dxux = VAH_TCD(UX, 1, fx); g.dxuy = VAH_TCD(UY, 1, fx); g.dxun = VAH_TCD(UN, 1, fx);
     g.dyut = VAH_TCD(UT, sy, fy); g.dyux = VAH_TCD(UX, sy, fy); g.dyuy = VAH_TCD(UY, sy, fy); g.dyun = VAH_TCD(UN, sy, fy);
     g.dxp = VAH_TCD(PP, 1, fx); g.dyp = VAH_TCD(PP, sy, fy);

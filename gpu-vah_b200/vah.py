@@ -81,7 +81,8 @@ EXPORTS = ["vah_version", "vah_eos_table_build", "vah_event_create", "vah_event_
            "vah_ic_longitudinal", "vah_event_autotune", "vah_batch_autotune",
            "vah_batch_freezeout_volume", "vah_batch_fallback_mask", "vah_event_set_validity",
            "vah_event_get_validity", "vah_batch_add_glauber", "vah_ic_mc_glauber_participants",
-           "vah_event_track_fallbacks", "vah_event_get_fallback_mask", "vah_fp64_peak"]
+           "vah_event_track_fallbacks", "vah_event_get_fallback_mask", "vah_fp64_peak", "vah_event_init_glauber",
+           "vah_event_init_optical_glauber"]
 
 _lib = None
 
@@ -221,6 +222,21 @@ class Event:
         a = np.ascontiguousarray(e_interior, dtype=np.float64)
         check(self.L.vah_event_init_from_e(self.ev, t0, a.ctypes.data_as(P), pl_mode), "vah_event_init_from_e")
 
+    def init_glauber(self, t0, b, seed, e_peak, e_floor=1e-3, sigma_nn_fm2=4.2, A=197, R=6.38, a=0.535, width=0.5,
+                     eta_flat=1.5, sigma_eta=1.3, pl_mode=VAH_PL_ISOTROPIC):
+        """MC-Glauber initial state generated on the device (vah_event_init_glauber)."""
+        g = Glauber(b, sigma_nn_fm2, A, R, a, width, seed, e_peak, e_floor, eta_flat, sigma_eta)
+        self.L.vah_event_init_glauber.argtypes = [C.c_void_p, D, C.POINTER(Glauber), I]
+        check(self.L.vah_event_init_glauber(self.ev, t0, C.byref(g), pl_mode), "vah_event_init_glauber")
+
+    def init_optical_glauber(self, t0, b, e_peak, e_floor=1e-3, sigma_nn_fm2=4.2, A=197, R=6.38, a=0.535,
+                             x_coll=0.15, eta_flat=1.5, sigma_eta=1.3, pl_mode=VAH_PL_ISOTROPIC):
+        """Optical-Glauber initial state generated on the device (vah_event_init_optical_glauber)."""
+        o = Optical(b, sigma_nn_fm2, A, R, a, x_coll, e_peak, e_floor, eta_flat, sigma_eta)
+        self.L.vah_event_init_optical_glauber.argtypes = [C.c_void_p, D, C.POINTER(Optical), I]
+        check(self.L.vah_event_init_optical_glauber(self.ev, t0, C.byref(o), pl_mode),
+              "vah_event_init_optical_glauber")
+
     def set_ghost_cells(self):
         check(self.L.vah_event_set_ghost_cells(self.ev), "vah_event_set_ghost_cells")
 
@@ -312,6 +328,11 @@ def _batch_lib():
 class Glauber(C.Structure):
     _fields_ = [("b", D), ("sigma_nn_fm2", D), ("A", I), ("ws_R", D), ("ws_a", D), ("width", D),
                 ("seed", C.c_ulonglong), ("e_peak", D), ("e_floor", D), ("eta_flat", D), ("sigma_eta", D)]
+
+
+class Optical(C.Structure):
+    _fields_ = [("b", D), ("sigma_nn_fm2", D), ("A", I), ("ws_R", D), ("ws_a", D), ("x_coll", D), ("e_peak", D),
+                ("e_floor", D), ("eta_flat", D), ("sigma_eta", D)]
 
 
 class Batch:

@@ -312,9 +312,12 @@ int vah_batch_remove(vah_batch *b, int slot);
 /* An event whose initial energy density is generated on the device (no
  * reference counterpart; the reference builds ICs on the host,
  * InitialConditions.cpp:196-292): the MC-Glauber collision of
- * vah_ic_mc_glauber (participants sampled on the host, their Gaussians
- * deposited on the GPU), e(x, y, eta) = e_peak v(x,y) / max v * f(eta) +
- * e_floor with f from vah_ic_longitudinal (1 in 2+1D); then as vah_batch_add. */
+ * vah_ic_mc_glauber, computed on the GPU (one block samples both nuclei with
+ * the host sampler's random streams and keeps the participants in its order;
+ * a grid deposits their Gaussians), e(x, y, eta) = e_peak v(x,y) / max v *
+ * f(eta) + e_floor with f vah_ic_longitudinal's profile (1 in 2+1D); then as
+ * vah_batch_add. Positions and e agree with the host generator to rounding
+ * (the GPU's exp, sin, cos). A <= 256; VAH_ERR_ARG otherwise. */
 typedef struct vah_glauber {
     double b, sigma_nn_fm2;
     int A;
@@ -325,6 +328,25 @@ typedef struct vah_glauber {
 } vah_glauber;
 int vah_batch_add_glauber(vah_batch *b, const vah_lattice *lat, const vah_hydro *hydro, double dt,
                           const vah_glauber *g, int pl_mode, int *slot);
+/* The same MC-Glauber initial state generated on the device straight into an
+ * event (vah_event_init_from_e with the generated e; nothing crosses to or
+ * from the host). */
+int vah_event_init_glauber(vah_event *ev, double t0, const vah_glauber *g, int pl_mode);
+/* The optical Glauber profile of vah_ic_optical_glauber, generated on the
+ * device into an event: the Woods-Saxon thickness table by Simpson in z (a
+ * thread per radius, 2048 radii), its normalisation to A nucleons, then
+ * (1 - x_coll) N_part/2 + x_coll N_coll per transverse cell, e = e_peak v /
+ * max v * f(eta) + e_floor with f as above. Where no nucleon pair overlaps
+ * (max v = 0) the event holds the flat floor e_floor (the host generator
+ * returns VAH_ERR_ARG there). */
+typedef struct vah_optical {
+    double b, sigma_nn_fm2;
+    int A;
+    double ws_R, ws_a, x_coll;
+    double e_peak, e_floor;
+    double eta_flat, sigma_eta;
+} vah_optical;
+int vah_event_init_optical_glauber(vah_event *ev, double t0, const vah_optical *o, int pl_mode);
 /* nsteps RK2 steps of every admitted event (asynchronous). */
 int vah_batch_step(vah_batch *b, int nsteps);
 int vah_batch_sync(vah_batch *b);

@@ -51,13 +51,15 @@ void tile_stage(TileHost *h, int stage, double t, double dt) {
                     const double ux = Uin[1][s], uy = Uin[2][s];
                     float H[NQ];
                     const unsigned f = vah::tile_face<PHYS>(qa, s, strides[d], d, t_src, (double)Ein[s],
-                                                            std::sqrt(std::fabs(ux * ux + uy * uy)), H);
+                                                            std::sqrt(std::fabs(ux * ux + uy * uy)), H, 1);
                     h->counters[0] += f & 255u;
                     for (int n = 0; n < NQ; ++n) h->H[d][n][s] = H[n];
                 }
     vah::TilePrims pr;
     pr.E = Ein;
     pr.P = Pin;
+    pr.psy = sy;
+    pr.psz = sz;
     for (int m = 0; m < 4; ++m) {
         pr.U[m] = Uin[m];
         pr.UP[m] = Uup[m];
@@ -77,9 +79,10 @@ void tile_stage(TileHost *h, int stage, double t, double dt) {
                 }
                 float val[NQ], e, p, u[4];
                 int bad = 0;
-                const int st = vah::tile_cell<PHYS, IS3D>(qa, s, sy, sz, pr, s, sy, sz, flux, qavg, stage == 2,
-                                                         h->eos, t_src, t_inv, dt, h->dx, h->dy, h->dz, h->etabar,
-                                                         val, e, p, u, nullptr, bad);
+                pr.pi = s;
+                const int st = vah::tile_cell<PHYS, IS3D>(qa, s, sy, sz, pr, s, flux, qavg, stage == 2, h->eos, t_src,
+                                                         t_inv, dt, h->dx, h->dy, h->dz, h->etabar, val, e, p, u,
+                                                         nullptr, bad);
                 if (st != 0) h->counters[1]++;
                 if (bad || st == 2) h->counters[2]++;
                 for (int n = 0; n < NQ; ++n) outv[n * h->ncell + s] = val[n];
