@@ -112,15 +112,16 @@ def test_gpu_fallbacks_fire_and_match_the_oracle_cell_by_cell():
     state. Then, at every step up to 200:
       * the fallback masks of both stages equal the oracle's cell by cell, and
         so do the cell-fallback counts, at every step of the run;
-      * the face-fallback count stays within 1% of the oracle's x + y count
+      * the face-fallback count stays within 1e-4 of the oracle's x + y count
         (in 2+1D the reference also inverts the eta faces, whose fluxes are
         exact zeros; the library skips them): a face inversion in the dilute
         floor can sit on the edge of the reference's fallback test, where the
         device's fused multiply-adds and refined hardware reciprocal move the
         Newton iterates' last bits; the differences are printed;
       * away from fallback cells and their neighbours e and P_L agree within
-        1e-8 and u^mu within 1e-7, normwise (measured worst over the run: about
-        1.3e-9 and 8e-9). A face inversion that falls back in one code only (the
+        1e-8 and u^mu within 1e-7, normwise (measured worst over the run: 4.7e-9
+        and 1.3e-8; face fallbacks 2153379 against the oracle's 2153381, one
+        step of 200 differing). A face inversion that falls back in one code only (the
         face counts above) changes the fluxes of the face's two cells, and the
         inversion near P_L -> 0 amplifies last-bit differences of its input;
         both sit in the dilute floor, far below the peak."""
@@ -172,7 +173,7 @@ def test_gpu_fallbacks_fire_and_match_the_oracle_cell_by_cell():
           f"free run {worst['free']:.2e}; per step e, P_L {worst['e_pl']:.2e}, u {worst['u']:.2e}; "
           f"face fallbacks {face_gpu} (oracle x+y {face_oracle}), {face_steps_differing} of 200 steps differ")
     assert cells_fell > 10000 and st[1] > 1000  # fallbacks fired and kept firing
-    assert abs(face_gpu - face_oracle) <= 0.01 * face_oracle + 10, (face_gpu, face_oracle)
+    assert abs(face_gpu - face_oracle) <= 1e-4 * face_oracle + 10, (face_gpu, face_oracle)
     ev.close()
 
 
