@@ -12,15 +12,18 @@
 //
 // Structure: a persistent grid (2 blocks of 256 threads per SM) takes tiles
 // from a work-list through an atomic counter. For each tile one thread issues
-// a single 4-D TMA load (cp.async.bulk.tensor: x, y, z and all N_q fields) of
-// the tile plus a 2-cell halo of the stage-input conserved fields into shared
-// memory, completed on an mbarrier. The faces of the tile are then evaluated
-// once each into registers and shared memory (x: in registers, exchanged with
-// the neighbour cell through warp shuffles; y and z: a shared face buffer; the
-// tile's lower boundary faces: a second small buffer), every cell takes its
-// flux differences from there, and runs sources, inversion and regulator.
-// Face fluxes never leave the SM. Primitive fields (e, p, u), needed at +-1,
-// are read through L1.
+// a 4-D TMA load (cp.async.bulk.tensor: x, y, z and all N_q fields) of the
+// tile plus a 2-cell halo of the stage-input conserved fields into shared
+// memory, and two more of e, p and u^mu with a 1-cell halo, completed on an
+// mbarrier. The faces of the tile are then evaluated once each into registers
+// and shared memory (x: in registers, exchanged with the neighbour cell
+// through warp shuffles; y and z: a shared face buffer; the tile's lower
+// boundary faces: a second small buffer, evaluated by threads 0-127 in the
+// first of the two face phases so that every thread evaluates at most four
+// faces), every cell takes its flux differences from there and runs its
+// explicit update. Then the next tile's copies are issued, and they land
+// while this tile's cells run their FP64 inversions, regulator and stores.
+// Face fluxes never leave the SM.
 //
 // Tiles: 8x8x4 cells for 3+1D events (TMA box 12x12x8 x N_q), 16x16x1 for
 // 2+1D (box 20x20x1 x N_q). Buffers use a row pitch padded to 4 floats
@@ -49,7 +52,7 @@ struct TileShape {
     static constexpr int NBX = TY * TZ, NBY = TX * TZ, NBZ = IS3D ? TX * TY : 0;  // lower boundary faces per axis
     static constexpr int NBXY = NBX + NBY;
     static_assert(TX * TY * TZ == kTileThreads, "one thread per cell");
-    static_assert(NBXY <= kTileThreads && NBZ <= NBXY, "boundary faces: one per thread, z reusing the x/y buffer");
+    static_assert(NBXY + NBZ <= kTileThreads, "boundary faces: one per thread, all in the first face phase");
     static_assert((BX * 4) % 16 == 0, "TMA box rows must be a multiple of 16 bytes");
 };
 
@@ -161,7 +164,8 @@ __device__ __forceinline__ void tile_count(unsigned long long *c, unsigned v) {
 
 // The dynamic shared memory of one block: the TMA boxes (conserved fields,
 // then e, p, u), the face buffer of the +1/2 faces along y, then z, the lower
-// boundary faces (x and y, then z), and the mbarrier and the tile index.
+// boundary faces (x and y; z), and the mbarrier and the tile index. 3+1D with
+// N_q = 16: 115.6 KB, so that two blocks share an SM's 228 KB.
 template <int PHYS, bool IS3D>
 struct TileSmem {
     using SH = TileShape<IS3D>;
@@ -172,7 +176,7 @@ struct TileSmem {
     static constexpr size_t ep_floats = pad32((size_t)SH::PBOXN * 2);
     static constexpr size_t u_floats = pad32((size_t)SH::PBOXN * 4);
     static constexpr size_t face_floats = (size_t)kTileThreads * NQ;
-    static constexpr size_t bnd_floats = (size_t)SH::NBXY * NQ;
+    static constexpr size_t bnd_floats = (size_t)(SH::NBXY + SH::NBZ) * NQ;
     static constexpr size_t box_bytes = (size_t)SH::BOXN * NQ * 4, ep_bytes = (size_t)SH::PBOXN * 2 * 4,
                             u_bytes = (size_t)SH::PBOXN * 4 * 4;  // what the copies write
     static constexpr size_t bar_offset =
@@ -196,7 +200,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     float *sP = sQ + SM::box_floats;           // [2][PBZ][PBY][PBX]: e, p
     float *sU = sP + SM::ep_floats;            // [4][PBZ][PBY][PBX]: ut, ux, uy, un
     float *sF = sU + SM::u_floats;             // [NQ][256]: +1/2 faces along y, then z
-    float *sB = sF + SM::face_floats;          // [NQ][NBXY]: lower boundary faces (x, y; then z)
+    float *sB = sF + SM::face_floats;          // [NQ][NBXY], [NQ][NBZ]: lower boundary faces (x, y; z)
     unsigned long long *bar = (unsigned long long *)((char *)tile_smem + SM::bar_offset);
     int &s_item = *(int *)(bar + 1);
     const float *const sE = sP, *const sPp = sP + PBOXN, *const sUX = sU + PBOXN, *const sUY = sU + 2 * PBOXN;
@@ -214,36 +218,33 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     __syncthreads();
     unsigned phase = 0;
 
-    for (;;) {
-        if (tid == 0) s_item = (int)atomicAdd(next_item, 1u);
-        __syncthreads();
-        const int w = s_item;
-        if (w >= nitems) break;
+    // the stage inputs of tile w: conserved fields (halo 2), e and p, u (halo 1)
+    auto issue = [&](int w) {
+        const TileItem it = items[w];
+        const TileSlot &d = slots[it.slot];
+        const int par = clk ? clk[it.slot].parity : clk0.parity;
+        fence_proxy_async_smem();  // the previous tile's generic reads of these buffers come first
+        mbar_expect_tx(bar, (unsigned)(SM::box_bytes + SM::ep_bytes + SM::u_bytes));
+        const int z0 = IS3D ? it.k0 : 2, pz0 = IS3D ? it.k0 + 1 : 2;
+        tma_load_4d(sQ, &d.tmQ[stage == 1 ? 0 : 1], bar, it.i0, it.j0, z0, 0);
+        tma_load_4d(sP, &d.tmEP[stage == 1 ? 0 : 1], bar, it.i0, it.j0 + 1, pz0, 0);
+        tma_load_4d(sU, &d.tmU[stage == 1 ? par : 2], bar, it.i0, it.j0 + 1, pz0, 0);
+    };
+    if (tid == 0) {
+        s_item = (int)atomicAdd(next_item, 1u);
+        if (s_item < nitems) issue(s_item);
+    }
+    __syncthreads();
+    int w = s_item;
+
+    while (w < nitems) {
         const TileItem it = items[w];
         const TileSlot &d = slots[it.slot];
         const TileClock c = clk ? clk[it.slot] : clk0;  // clk0, dt0: a single event's clock and step, by value
         const double dt = clk ? d.dt : dt0;
-        float *const *u_n = c.parity ? d.uB : d.uA;      // u^n
-        float *const *u_p = c.parity ? d.uA : d.uB;      // u^{n-1}
-        // stage inputs and outputs (FullyDiscreteKurganovTadmorScheme.cpp:761-789)
-        float *Qout = d.Q[stage == 1 ? 1 : 0];
-        float *Eout = d.ep[stage == 1 ? 1 : 0][0], *Pout_p = d.ep[stage == 1 ? 1 : 0][1];
-        float *const *Uup = stage == 1 ? u_p : u_n;  // previous-stage u (d_tau u)
-        float *const *Uout = stage == 1 ? d.uS : u_p;
-        const long long fs = d.fstride;
-        const int pitch = d.pitch;
-        const long long plane = (long long)pitch * d.ncy;
         const double t_src = stage == 1 ? c.t : c.t + dt;
         const double t_inv = c.t + dt;
 
-        if (tid == 0) {  // the stage inputs: conserved fields (halo 2), e and p, u (halo 1)
-            fence_proxy_async_smem();  // the previous tile's generic reads of these buffers come first
-            mbar_expect_tx(bar, (unsigned)(SM::box_bytes + SM::ep_bytes + SM::u_bytes));
-            const int z0 = IS3D ? it.k0 : 2, pz0 = IS3D ? it.k0 + 1 : 2;
-            tma_load_4d(sQ, &d.tmQ[stage == 1 ? 0 : 1], bar, it.i0, it.j0, z0, 0);
-            tma_load_4d(sP, &d.tmEP[stage == 1 ? 0 : 1], bar, it.i0, it.j0 + 1, pz0, 0);
-            tma_load_4d(sU, &d.tmU[stage == 1 ? c.parity : 2], bar, it.i0, it.j0 + 1, pz0, 0);
-        }
         if (!mbar_wait(bar, phase, 1u << 22)) {
             if (tid == 0) atomicOr(err, kTileErrTimeout);
             // wait once more (bounded) so that no copy is left writing this block's memory
@@ -255,6 +256,8 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         // this thread's cell, in interior and ghosted coordinates, and in the boxes
         const int ci = it.i0 + lx, cj = it.j0 + ly, ck = it.k0 + lz;
         const bool live = ci < d.nx && cj < d.ny && ck < d.nz;
+        const int pitch = d.pitch;
+        const long long plane = (long long)pitch * d.ncy;
         const long long s = (ci + 2) + (long long)pitch * (cj + 2) + plane * (ck + 2);
         const int bc = (lx + 2) + BX * ((ly + 2) + BY * (IS3D ? lz + 2 : 0));
         const int pc = (lx + 2) + PBX * ((ly + 1) + PBY * (IS3D ? lz + 1 : 0));
@@ -268,14 +271,9 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         const double e0 = (double)sE[pc], ux0 = (double)sUX[pc], uy0 = (double)sUY[pc];
         const double uT0 = sqrt(fabs(ux0 * ux0 + uy0 * uy0));
 
-        // ---- faces: +1/2 along x (registers), the x and y lower boundary faces, +1/2 along y ----
-        float Hx[NQ];
-        if (live) count(tile_face<PHYS>(bq, bc, 1, 0, t_src, e0, uT0, Hx, 1));
-        else
-#pragma unroll
-            for (int n = 0; n < NQ; ++n) Hx[n] = 0.0f;
-        // lower boundary face b of the tile along `dir`; the left cell is in the halo
-        auto boundary = [&](int b, int dir, float *dst) {
+        // lower boundary face b of the tile along `dir` into dst (stride ds);
+        // the left cell is in the halo
+        auto boundary = [&](int b, int dir, float *dst, int ds) {
             int bi, bj, bk;  // left cell in the conserved box
             if (dir == 0) { bi = 1; bj = 2 + b % TY; bk = IS3D ? 2 + b / TY : 0; }
             else if (dir == 1) { bi = 2 + b % TX; bj = 1; bk = IS3D ? 2 + b / TX : 0; }
@@ -286,13 +284,25 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 const int pl = bi + PBX * ((bj - 1) + PBY * (IS3D ? bk - 1 : 0));
                 const double el = (double)sE[pl], ux = (double)sUX[pl], uy = (double)sUY[pl];
                 count(tile_face<PHYS>(bq, bi + BX * (bj + BY * bk), dir == 0 ? 1 : (dir == 1 ? SY : SZ), dir, t_src, el,
-                                      sqrt(fabs(ux * ux + uy * uy)), dst, SH::NBXY));
+                                      sqrt(fabs(ux * ux + uy * uy)), dst, ds));
             } else {
 #pragma unroll
-                for (int n = 0; n < NQ; ++n) dst[n * SH::NBXY] = 0.0f;
+                for (int n = 0; n < NQ; ++n) dst[n * ds] = 0.0f;
             }
         };
-        if (tid < SH::NBXY) boundary(tid < SH::NBX ? tid : tid - SH::NBX, tid < SH::NBX ? 0 : 1, sB + tid);
+
+        // ---- faces, phase 1: +1/2 along x (registers) and y (face buffer); the
+        // lower boundary faces along x and y (threads 0 .. NBXY-1) and, in
+        // 3+1D, along z (the next NBZ threads), so that no thread evaluates
+        // more than three faces in this phase and one in the next ----
+        float Hx[NQ];
+        if (live) count(tile_face<PHYS>(bq, bc, 1, 0, t_src, e0, uT0, Hx, 1));
+        else
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) Hx[n] = 0.0f;
+        if (tid < SH::NBXY) boundary(tid < SH::NBX ? tid : tid - SH::NBX, tid < SH::NBX ? 0 : 1, sB + tid, SH::NBXY);
+        else if (IS3D && tid < SH::NBXY + SH::NBZ)
+            boundary(tid - SH::NBXY, 2, sB + SH::NBXY * NQ + (tid - SH::NBXY), SH::NBZ);
         if (live) count(tile_face<PHYS>(bq, bc, SY, 1, t_src, e0, uT0, sF + tid, kTileThreads));
         else
 #pragma unroll
@@ -310,17 +320,17 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             const float ym = ly > 0 ? sF[n * kTileThreads + tid - TX] : sB[n * SH::NBXY + SH::NBX + lx + TX * lz];
             flux[n] = cx * (hm - Hx[n]) + cy * (ym - sF[n * kTileThreads + tid]);
         }
-        if (IS3D) {  // +1/2 along z and the z lower boundary faces (reusing the buffers)
+        if (IS3D) {  // phase 2: +1/2 along z (reusing the face buffer)
             __syncthreads();
-            if (tid < SH::NBZ) boundary(tid, 2, sB + tid);
             if (live) count(tile_face<PHYS>(bq, bc, SZ, 2, t_src, e0, uT0, sF + tid, kTileThreads));
             else
 #pragma unroll
                 for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = 0.0f;
             __syncthreads();
+            const float *sBz = sB + SH::NBXY * NQ;
 #pragma unroll
             for (int n = 0; n < NQ; ++n) {
-                const float zm = lz > 0 ? sF[n * kTileThreads + tid - TX * TY] : sB[n * SH::NBXY + lx + TX * ly];
+                const float zm = lz > 0 ? sF[n * kTileThreads + tid - TX * TY] : sBz[n * SH::NBZ + lx + TX * ly];
                 flux[n] += cz * (zm - sF[n * kTileThreads + tid]);
             }
         }
@@ -329,30 +339,48 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             tile_count(d.counters + 2, fnan ? 1u : 0u);
         }
 
-        // ---- the cell ----
-        if (live) {
-            TilePrims pr;
-            pr.E = sE;
-            pr.P = sPp;
+        // ---- the cell: the explicit update (the last reads of the boxes) ----
+        float *const *u_n = c.parity ? d.uB : d.uA;  // u^n
+        float *const *u_p = c.parity ? d.uA : d.uB;  // u^{n-1}
+        TilePrims pr;
+        pr.E = sE;
+        pr.P = sPp;
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                pr.U[m] = sU + m * PBOXN;
-                pr.UP[m] = Uup[m];
-                pr.G[m] = u_n[m];
-            }
-            pr.pi = pc;
-            pr.psy = PSY;
-            pr.psz = PSZ;
+        for (int m = 0; m < 4; ++m) {
+            pr.U[m] = sU + m * PBOXN;
+            pr.UP[m] = stage == 1 ? u_p[m] : u_n[m];  // previous-stage u (d_tau u)
+            pr.G[m] = u_n[m];
+        }
+        pr.pi = pc;
+        pr.psy = PSY;
+        pr.psz = PSZ;
+        float val[NQ], e_prev = 0.0f;
+        int bad = 0;
+        if (live)
+            tile_cell_explicit<PHYS, IS3D>(bq, bc, SY, SZ, pr, s, flux, eos, t_src, dt, d.dx, d.dy, d.dz, d.etabar, val,
+                                           e_prev, bad);
+
+        // every read of this tile's boxes is done: the next tile's copies
+        // overlap this tile's inversions, regulator and stores
+        if (tid == 0) {
+            s_item = (int)atomicAdd(next_item, 1u);
+            if (s_item < nitems) issue(s_item);
+        }
+        __syncthreads();
+        const int w_next = s_item;
+
+        // ---- the cell: inversion, regulator, stores (stage outputs:
+        // FullyDiscreteKurganovTadmorScheme.cpp:761-789) ----
+        if (live) {
+            const long long fs = d.fstride;
             struct {
                 const float *q;
                 long long fs;
                 __device__ float operator()(int n, long long i) const { return q[n * fs + i]; }
             } qavg{d.Q[0], fs};
-            float val[NQ], e, p, u[4], rmap[11];
-            int bad = 0;
-            const int st = tile_cell<PHYS, IS3D>(bq, bc, SY, SZ, pr, s, flux, qavg, stage == 2, eos, t_src, t_inv, dt,
-                                                 d.dx, d.dy, d.dz, d.etabar, val, e, p, u,
-                                                 d.regmap[0] ? rmap : nullptr, bad);
+            float e, p, u[4], rmap[11];
+            const int st = tile_cell_invert<PHYS>(pr, s, qavg, stage == 2, eos, t_inv, e_prev, val, e, p, u,
+                                                  d.regmap[0] ? rmap : nullptr);
             if (d.regmap[0] && Phys<PHYS>::PIMUNU)
                 for (int m = 0; m < 11; ++m) d.regmap[m][s] = (double)rmap[m];
             if (d.counters) {
@@ -369,6 +397,9 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 }
             }
             // stores, and the face ghost layers of boundary cells (setGhostCellsKernelI/J/K)
+            float *Qout = d.Q[stage == 1 ? 1 : 0];
+            float *Eout = d.ep[stage == 1 ? 1 : 0][0], *Pout_p = d.ep[stage == 1 ? 1 : 0][1];
+            float *const *Uout = stage == 1 ? d.uS : u_p;
             const long long sy = pitch, sz = plane;
             auto store = [&](long long at) {
 #pragma unroll
@@ -386,7 +417,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             if (ck == 0) { store(s - sz); store(s - 2 * sz); }
             if (ck == d.nz - 1) { store(s + sz); store(s + 2 * sz); }
         }
-        __syncthreads();  // every read of this tile's buffers is done
+        w = w_next;
     }
 }
 

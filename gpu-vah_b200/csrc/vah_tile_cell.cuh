@@ -84,18 +84,17 @@ struct TilePrims {
     const float *UP[4], *G[4];
 };
 
-// The cell part of a stage (eulerStepKernelSource, the axis sources,
-// [the convex combination], setInferredVariablesKernel, the regulator):
-// q: the stage-input conserved fields at box index b (strides bsy, bsz);
-// pr: the primitives; s: the cell's global index; flux[n]: the flux
-// differences dt/h (H(-1/2) - H(+1/2)) summed over the axes; qavg(n, s): q^n
-// (stage 2). Writes the new conserved values, e, p, u; returns the inversion's
-// status (0 converged, 1 fallback, 2 NaN) and sets bad when a source is NaN.
-template <int PHYS, bool IS3D, typename QA, typename QV>
-VAH_HD int tile_cell(const QA &q, long long b, long long bsy, long long bsz, const TilePrims &pr, long long s,
-                     const float *flux, const QV &qavg, bool stage2, const Eos &eos, double t_src, double t_inv,
-                     double dt, double dx, double dy, double dz, double etabar, float *val, float &e, float &p,
-                     float *u, float *rmap, int &bad) {
+// The explicit part of a cell's stage (eulerStepKernelSource and the axis
+// sources): q: the stage-input conserved fields at box index b (strides bsy,
+// bsz); pr: the primitives; s: the cell's global index; flux[n]: the flux
+// differences dt/h (H(-1/2) - H(+1/2)) summed over the axes. Writes the
+// updated conserved values to val and the cell's e (the inversion's fallback
+// energy) to e_prev; sets bad when a source is NaN. The last part of the
+// stage that reads q and the primitives around the cell.
+template <int PHYS, bool IS3D, typename QA>
+VAH_HD void tile_cell_explicit(const QA &q, long long b, long long bsy, long long bsz, const TilePrims &pr,
+                               long long s, const float *flux, const Eos &eos, double t_src, double dt, double dx,
+                               double dy, double dz, double etabar, float *val, float &e_prev, int &bad) {
     constexpr int NQ = Phys<PHYS>::NQ;
     float qc[NQ];
 #pragma unroll
@@ -151,6 +150,18 @@ VAH_HD int tile_cell(const QA &q, long long b, long long bsy, long long bsz, con
             for (int n = 0; n < 4; ++n) val[n] += dtf * Sa[n];
         }
     }
+    e_prev = g.e;
+}
+
+// The rest of the cell's stage ([the convex combination],
+// setInferredVariablesKernel, the regulator) from tile_cell_explicit's
+// results, reading nothing around the cell: qavg(n, s) = q^n (stage 2), the
+// Newton guess from pr.G at s. Writes the new conserved values (val), e, p,
+// u; returns the inversion's status (0 converged, 1 fallback, 2 NaN).
+template <int PHYS, typename QV>
+VAH_HD int tile_cell_invert(const TilePrims &pr, long long s, const QV &qavg, bool stage2, const Eos &eos,
+                            double t_inv, float e_prev, float *val, float &e, float &p, float *u, float *rmap) {
+    constexpr int NQ = Phys<PHYS>::NQ;
     if (stage2) {  // Q = (q^n + Q*) / 2
 #pragma unroll
         for (int n = 0; n < NQ; ++n) val[n] = (val[n] + qavg(n, s)) * 0.5f;
@@ -160,12 +171,25 @@ VAH_HD int tile_cell(const QA &q, long long b, long long bsy, long long bsz, con
     double qd[16], prim[6];
 #pragma unroll
     for (int n = 0; n < 16; ++n) qd[n] = n < NQ ? (double)val[n] : 0.0;
-    const int st = invert<PHYS>(eos, t_inv, qd, (double)g.e, sqrt(fabs(gx * gx + gy * gy)), prim);
+    const int st = invert<PHYS>(eos, t_inv, qd, (double)e_prev, sqrt(fabs(gx * gx + gy * gy)), prim);
     e = (float)prim[0];
     p = (float)prim[1];
     for (int m = 0; m < 4; ++m) u[m] = (float)prim[2 + m];
     regulate<PHYS>((float)t_inv, e, p, val, u, rmap);
     return st;
+}
+
+// The whole cell part of a stage (eulerStepKernelSource, the axis sources,
+// [the convex combination], setInferredVariablesKernel, the regulator), as
+// the two parts above.
+template <int PHYS, bool IS3D, typename QA, typename QV>
+VAH_HD int tile_cell(const QA &q, long long b, long long bsy, long long bsz, const TilePrims &pr, long long s,
+                     const float *flux, const QV &qavg, bool stage2, const Eos &eos, double t_src, double t_inv,
+                     double dt, double dx, double dy, double dz, double etabar, float *val, float &e, float &p,
+                     float *u, float *rmap, int &bad) {
+    float e_prev;
+    tile_cell_explicit<PHYS, IS3D>(q, b, bsy, bsz, pr, s, flux, eos, t_src, dt, dx, dy, dz, etabar, val, e_prev, bad);
+    return tile_cell_invert<PHYS>(pr, s, qavg, stage2, eos, t_inv, e_prev, val, e, p, u, rmap);
 }
 
 
