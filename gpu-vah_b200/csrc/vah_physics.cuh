@@ -18,6 +18,31 @@
 #define VAH_HD inline
 #endif
 
+namespace vah {
+
+// f / d. On the device: the hardware reciprocal estimate (rcp.approx, about
+// 20 good bits) refined by one Newton-Raphson step y += y (1 - d y), i.e. to
+// about 2^-40 relative (measured: 9.8e-13, vah_math_check), times f -- three
+// dependent operations instead of an IEEE division. The estimate flushes
+// subnormal inputs and results (.ftz), so outside |d| in [2^-1000, 2^1001)
+// -- an exponent test on the integer pipe, essentially never taken -- the
+// result is the IEEE quotient (a NaN or infinite d lands there too). On the
+// host: the IEEE quotient.
+VAH_HD double quotient_fast(double f, double d) {
+#ifdef __CUDA_ARCH__
+    const unsigned biased = ((unsigned)__double2hiint(d) >> 20) & 0x7ffu;
+    if (biased - 23u > 2000u) return f / d;
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    y = fma(y, fma(-d, y, 1.0), y);
+    return f * y;
+#else
+    return f / d;
+#endif
+}
+
+}  // namespace vah
+
 #include "vah_closure_polys.h"
 
 namespace vah {
@@ -30,6 +55,11 @@ struct Phys {
     static constexpr bool PIMUNU = PHYS != kIdeal;
     static constexpr bool BULK = PHYS == kPimunuPi;
 };
+
+// The FP32 form (R = float) takes closure-fit quotients and the face
+// states' divisions through quotient_fast; the FP64 form keeps IEEE divisions.
+template <typename R>
+constexpr bool kFastQuot = sizeof(R) == 4;
 
 constexpr int kSlotPL = 4;
 constexpr int kSlotPi = 15;
@@ -244,7 +274,7 @@ struct InvSetup {
     double G0, G1;
 };
 
-template <int PHYS>
+template <int PHYS, bool FAST = false>
 VAH_HD void invert_setup(double t, const double *q, InvSetup &s) {
     double pitt = 0, pitx = 0, pity = 0, pitn = 0, bulk = 0;
     if (Phys<PHYS>::PIMUNU) {
@@ -258,7 +288,7 @@ VAH_HD void invert_setup(double t, const double *q, InvSetup &s) {
     const double m0 = q[0] - pitt, m1 = q[1] - pitx, m2 = q[2] - pity, m3 = q[3] - pitn;
     double m0pl = m0 + pl;
     if (m0pl == 0.0) m0pl = 1.e-16;
-    const double F = m3 / m0pl;  // W off: F = A
+    const double F = FAST ? quotient_fast(m3, m0pl) : m3 / m0pl;  // W off: F = A
     const double Ft = t * F;
     const double Ft2 = Ft * Ft;
     const double x = sqrt(fabs(1. - Ft2));
@@ -281,29 +311,10 @@ VAH_HD void invert_setup(double t, const double *q, InvSetup &s) {
     s.G1 = 0.5 * s.b * s.bT;
 }
 
-// The Newton correction f / fp. On the device: the hardware reciprocal
-// estimate (rcp.approx, about 20 good bits) refined by one Newton-Raphson
-// step y += y (1 - fp y), i.e. to about 2^-40 relative (measured: 9.8e-13,
-// vah_math_check), times f -- three dependent operations instead of an IEEE
-// division. The correction only needs
-// to be accurate relative to itself: where the iteration stops it is ~1e-7 of
-// u_T, so its error moves the root by ~1e-21 relative. The estimate flushes
-// subnormal inputs and results (.ftz), so outside |fp| in [2^-1000, 2^1001)
-// -- an exponent test on the integer pipe, essentially never taken -- the
-// correction is the IEEE quotient, as in the reference (a NaN or infinite fp
-// lands there too).
-VAH_HD double newton_correction(double f, double fp) {
-#ifdef __CUDA_ARCH__
-    const unsigned biased = ((unsigned)__double2hiint(fp) >> 20) & 0x7ffu;
-    if (biased - 23u > 2000u) return f / fp;
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(fp));
-    y = fma(y, fma(-fp, y, 1.0), y);
-    return f * y;
-#else
-    return f / fp;
-#endif
-}
+// The Newton correction f / fp through quotient_fast. It only needs to be
+// accurate relative to itself: where the iteration stops it is ~1e-7 of u_T,
+// so its error (about 1e-12) moves the root by ~1e-19 relative.
+VAH_HD double newton_correction(double f, double fp) { return quotient_fast(f, fp); }
 
 // Newton iteration for u_T from the guess uT0 (EnergyMomentumTensor.cpp:30-72).
 // Returns 0 with the root in uT, or 1 when the reference falls back.
@@ -444,13 +455,15 @@ VAH_HD int face_velocity(const InvSetup &s, double ePrev, double uT0, int dir, d
 // fallback energy and Newton guess.
 // Returns the number of the two inversions that fell back; bit 8 flags a NaN.
 // The velocity of a converged solve, as face_velocity (status 0 or 2).
+template <bool FAST = false>
 VAH_HD int face_velocity_of(const InvSetup &s, double uT, int dir, double *v) {
     double vv;
     if (dir == 2) {
         vv = s.F;
     } else {
         // uT m x / (mbt C), C = sqrt(1 + uT^2), with 1/C from rsqrt_d
-        vv = uT * (dir == 0 ? s.m1 : s.m2) * s.x * rsqrt_d(1.0 + uT * uT) / s.mbt;
+        const double num = uT * (dir == 0 ? s.m1 : s.m2) * s.x * rsqrt_d(1.0 + uT * uT);
+        vv = FAST ? quotient_fast(num, s.mbt) : num / s.mbt;
     }
     *v = vv;
     return (isnan(vv) || isnan(s.c0)) ? 2 : 0;
@@ -651,10 +664,10 @@ VAH_HD int cell_sources(const Eos &eos, const R *Q, const CellGradT<R> &g, const
 #pragma unroll
     for (int k = 2; k < 16; ++k) ap[k] = ap[k - 1] * ap[1];
     const R a = R(ap[1]);
-    const R Rtilde = R(poly::Rtilde(ap));
-    const R Rbar0 = R(poly::Rbar0(ap));
-    const R Rgamma = R(poly::Rgamma(ap));
-    const R Rbar0P = R(poly::Rbar0P(ap));
+    const R Rtilde = R(poly::Rtilde<double, kFastQuot<R>>(ap));
+    const R Rbar0 = R(poly::Rbar0<double, kFastQuot<R>>(ap));
+    const R Rgamma = R(poly::Rgamma<double, kFastQuot<R>>(ap));
+    const R Rbar0P = R(poly::Rbar0P<double, kFastQuot<R>>(ap));
 
     const R e3p = e - 3 * p;
     const R ptHat = (e - pl - Rbar0 * e3p) * R(0.5);
@@ -703,16 +716,16 @@ VAH_HD int cell_sources(const Eos &eos, const R *Q, const CellGradT<R> &g, const
         if (third == R(0.0)) third = R(1.e-16);
         const R meq2 = 36 * third;
         const R z2logz = -2 * (1 + R(0.02536) * meq2);
-        const R g40 = (R(poly::g0m2040DividedBym2LogZTerm(ap)) * z2logz + R(poly::g0m2040DividedBym2Zm2Term(ap))) /
+        const R g40 = (R(poly::g0m2040DividedBym2LogZTerm<double, kFastQuot<R>>(ap)) * z2logz + R(poly::g0m2040DividedBym2Zm2Term<double, kFastQuot<R>>(ap))) /
                           meq2 +
-                      R(poly::g0m2040DividedBym2ConstantTerm(ap));
-        const R g20c = R(poly::g0m2020ConstantTerm(ap));
-        const R g20 = g20c + R(poly::g0m2020Z2LogZTerm(ap)) * z2logz + R(poly::g0m2020Z2Term(ap)) * meq2;
+                      R(poly::g0m2040DividedBym2ConstantTerm<double, kFastQuot<R>>(ap));
+        const R g20c = R(poly::g0m2020ConstantTerm<double, kFastQuot<R>>(ap));
+        const R g20 = g20c + R(poly::g0m2020Z2LogZTerm<double, kFastQuot<R>>(ap)) * z2logz + R(poly::g0m2020Z2Term<double, kFastQuot<R>>(ap)) * meq2;
         beta_lPi = 3 * g40;
         delta_lPi = g20 + g40;
         beta_PiPi = 1 - g20c;
         delta_PiPi = R(0.5) * (1 + g20c);
-        lambda_Pipi = div_const(3 * R(poly::G_G1(ap)), R(5.0), R(1.0) / R(5.0)) * (0 - cs2);
+        lambda_Pipi = div_const(3 * R(poly::G_G1<double, kFastQuot<R>>(ap)), R(5.0), R(1.0) / R(5.0)) * (0 - cs2);
     }
 
     const R dPL = -(pl - p) * taupiInv + zeta_zz * zDzu - zeta_zT * thetaT - beta_lPi * Pi * zDzu -
@@ -792,7 +805,7 @@ VAH_HD int cell_sources(const Eos &eos, const R *Q, const CellGradT<R> &g, const
     }
     if (BULK) {
         // SourceTerms.cpp:1030-1042
-        const R Rhat = R(poly::Rhat(ap));
+        const R Rhat = R(poly::Rhat<double, kFastQuot<R>>(ap));
         const R bb = R(1.0) / R(3.0) - cs2;
         const R tauPiInv = 15 * bb * bb * T / zeta_over_s(eos, T);
         const R zeta_z = div_const((Rhat - Rbar0) * e3p, R(3.0), R(1.0) / R(3.0));
@@ -821,10 +834,10 @@ VAH_HD void regulate(R t, R &e, R &p, R *q, const R *u, R *maps = nullptr) {
     const R pl = q[kSlotPL];
     double ap[9];  // FP64 closure fit, as in cell_sources
     ap[0] = 1.0;
-    ap[1] = (double)pl / (double)e;
+    ap[1] = kFastQuot<R> ? quotient_fast((double)pl, (double)e) : (double)pl / (double)e;
 #pragma unroll
     for (int k = 2; k < 9; ++k) ap[k] = ap[k - 1] * ap[1];
-    const R ptHat = (e - pl - R(poly::Rbar0(ap)) * (e - 3 * p)) * R(0.5);
+    const R ptHat = (e - pl - R(poly::Rbar0<double, kFastQuot<R>>(ap)) * (e - 3 * p)) * R(0.5);
     const R pitt = q[5], pitx = q[6], pity = q[7], pitn = q[8], pixx = q[9];
     const R pixy = q[10], pixn = q[11], piyy = q[12], piyn = q[13], pinn = q[14];
     const R ut = u[0], ux = u[1], uy = u[2], un = u[3];

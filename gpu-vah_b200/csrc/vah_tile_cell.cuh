@@ -39,7 +39,8 @@ struct ArrQ {
 // Kurganov-Tadmor flux through the face between cells L and L + st
 // (SemiDiscreteKurganovTadmorScheme.cpp:13-57, FluxLimiter.cpp:28-33): the
 // states reconstructed in FP32, inverted in FP64 from the guess uT (the left
-// cell's |u_T|), H[n hs] = wR qR + wL qL in FP32 (hs: the stride of the
+// cell's |u_T|; the setup's and the velocities' divisions through
+// quotient_fast), H[n hs] = wR qR + wL qL in FP32 (hs: the stride of the
 // destination, e.g. a shared face buffer). Returns the number of inversions
 // that fell back; bit 8 flags a NaN (ePrev: the left cell's e).
 template <int PHYS, typename QA>
@@ -60,13 +61,13 @@ VAH_TILE_FACE unsigned tile_face(const QA q, long long L, long long st, int dir,
         dL[n] = n < NQ ? (double)qL[n] : 0.0;
     }
     InvSetup sR, sL;
-    invert_setup<PHYS>(t, dR, sR);
-    invert_setup<PHYS>(t, dL, sL);
+    invert_setup<PHYS, true>(t, dR, sR);
+    invert_setup<PHYS, true>(t, dL, sL);
     double uR, uL, vR = 0.0, vL = 0.0;
     int nR, nL;
     newton_uT2(sR, sL, uT, uT, uR, uL, nR, nL);
-    const int stR = nR != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sR, uR, dir, &vR);
-    const int stL = nL != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sL, uL, dir, &vL);
+    const int stR = nR != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of<true>(sR, uR, dir, &vR);
+    const int stL = nL != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of<true>(sL, uL, dir, &vL);
     const double a = fmax(fabs(vL), fabs(vR));
     const float wR = (float)(0.5 * (vR - a)), wL = (float)(0.5 * (vL + a));
 #pragma unroll
