@@ -209,6 +209,12 @@ VAH_HD double eos_pressure(const Eos &eos, double e) {
     return table_lookup<true, false>(eos.tab, e).p;
 }
 
+// The same in FP32 arithmetic.
+VAH_HD float eos_pressure_f(const Eos &eos, float e) {
+    if (eos.kind == 0) return e / 3.0f;
+    return table_lookup<true, false>(eos.tab, e).p;
+}
+
 // (T, c_s^2); the conformal c_s^2 is the reference's integer `1/3` = 0
 // (EquationOfState.cpp:113).
 template <typename R>
@@ -390,8 +396,9 @@ VAH_HD void newton_uT2(const InvSetup &A, const InvSetup &B, double g0, double g
 }
 
 // The full inversion. Returns 0 (converged), 1 (fallback) or 2 (a NaN
-// reached e or u). out = {e, p, ut, ux, uy, un}.
-template <int PHYS>
+// reached e or u). out = {e, p, ut, ux, uy, un}. PF32 (the FP32 form): the
+// pressure from the EoS in FP32 arithmetic (the form stores p in FP32).
+template <int PHYS, bool PF32 = false>
 VAH_HD int invert(const Eos &eos, double t, const double *q, double ePrev, double uT0, double *out) {
     InvSetup s;
     invert_setup<PHYS>(t, q, s);
@@ -415,7 +422,7 @@ VAH_HD int invert(const Eos &eos, double t, const double *q, double ePrev, doubl
         ut = 1.0;
     }
     out[0] = e;
-    out[1] = eos_pressure(eos, e);
+    out[1] = PF32 ? (double)eos_pressure_f(eos, (float)e) : eos_pressure(eos, e);
     out[2] = ut;
     out[3] = ux;
     out[4] = uy;

@@ -167,12 +167,13 @@ VAH_HD int tile_cell_invert(const TilePrims &pr, long long s, const QV &qavg, bo
 #pragma unroll
         for (int n = 0; n < NQ; ++n) val[n] = (val[n] + qavg(n, s)) * 0.5f;
     }
-    // FP64 inversion from the previous-stage guess (EnergyMomentumTensor.cpp:74-197)
+    // FP64 inversion from the previous-stage guess (EnergyMomentumTensor.cpp:74-197);
+    // p = EoS(e) in FP32
     const double gx = (double)pr.G[1][s], gy = (double)pr.G[2][s];
     double qd[16], prim[6];
 #pragma unroll
     for (int n = 0; n < 16; ++n) qd[n] = n < NQ ? (double)val[n] : 0.0;
-    const int st = invert<PHYS>(eos, t_inv, qd, (double)e_prev, sqrt(fabs(gx * gx + gy * gy)), prim);
+    const int st = invert<PHYS, true>(eos, t_inv, qd, (double)e_prev, sqrt(fabs(gx * gx + gy * gy)), prim);
     e = (float)prim[0];
     p = (float)prim[1];
     for (int m = 0; m < 4; ++m) u[m] = (float)prim[2 + m];
