@@ -310,12 +310,14 @@ FP64_PEAK_TFLOPS = 64 * 2 * 148 * 1.965e9 / 1e12
 def fp64_roofline(cells, flux, precision, stage_s, peak=None):
     """FP64 FLOP/s of one RK stage against the FP64 peak (measured when given,
     else nominal), from the FLOP count per cell and stage in the committed ncu
-    summary."""
-    path = os.path.join(ROOT, "profiles", "split_stage_dram.json")
-    if flux != "per_cell" or not os.path.exists(path) or not stage_s:
+    summary (the FP32 form: the tile kernel's)."""
+    tile = precision == "fp32"
+    path = os.path.join(ROOT, "profiles", "tile_stage_dram.json" if tile else "split_stage_dram.json")
+    if (flux != "per_cell" and not tile) or not os.path.exists(path) or not stage_s:
         return None
     with open(path) as f:
-        per = json.load(f).get("fp64_flop_per_cell_per_stage", {}).get(precision)
+        d = json.load(f)
+    per = d.get("fp64_flop_per_cell_per_stage") if tile else d.get("fp64_flop_per_cell_per_stage", {}).get(precision)
     if not per:
         return None
     achieved = per * cells / stage_s / 1e12
@@ -330,7 +332,15 @@ def fp64_roofline(cells, flux, precision, stage_s, peak=None):
 
 def traffic_per_launch(cells, flux, precision):
     """DRAM bytes of one RK stage (its launches) from the committed ncu
-    summaries (bytes per interior cell, scaled to this event), or None."""
+    summaries (bytes per interior cell, scaled to this event), or None. The
+    FP32 form runs the tile kernel whatever the face option."""
+    if precision == "fp32":
+        path = os.path.join(ROOT, "profiles", "tile_stage_dram.json")
+        if not os.path.exists(path):
+            return None
+        with open(path) as f:
+            per = json.load(f).get("dram_bytes_per_cell_per_stage", {}).get("mean")
+        return per * cells if per else None
     if flux == "fused":
         name, key = "stage_kernel_dram.json", None
     elif flux == "per_cell":
@@ -717,14 +727,15 @@ def run_vah(args, rank, world, dist):
                          "frac": achieved / peak, "traffic": traffic_per_launch(cells, args.flux, args.precision),
                          "peak_kind": f"{peak_kind} copy bandwidth",
                          "algorithmic_bytes_per_cell_update": bpc,
-                         "kernel": ("stage_kernel (one fused RK stage)" if args.flux == "fused"
+                         "kernel": ("tile_kernel (one TMA-tiled launch per RK stage)" if prec == vah.VAH_FP32
+                                    else "stage_kernel (one fused RK stage)" if args.flux == "fused"
                                     else "one RK stage: face_kernel x3 + cell_kernel") + ", average over the two stages",
                          "avg_stage_ms": 1000 * avg_launch_s,
                          "fp64": fp64_roofline(cells, args.flux, args.precision, avg_launch_s, fp64_peak)},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
                     "path": "vah_rk2_step_host (pinned host state in, one step, state out)"},
-            "gpu_launches": launches * (1 if args.flux == "fused" else 4),
+            "gpu_launches": launches * (1 if args.flux == "fused" or prec == vah.VAH_FP32 else 4),
             "stats": {"face_fallbacks": stats.face_fallbacks, "cell_fallbacks": stats.cell_fallbacks,
                       "nan_cells": stats.nan_cells}}
     clk_summary = clk.summary()
@@ -738,7 +749,12 @@ def run_vah(args, rank, world, dist):
         form.update({"unit": "cell-updates/s", "dtype": "f32+f64-inversion" if other == vah.VAH_FP32 else "f64",
                      "ratio_to_headline": form["value"] / value,
                      "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                  "traffic": traffic_per_launch(cells, args.flux,
+                                                                "fp32" if other == vah.VAH_FP32 else "fp64"),
                                   "algorithmic_bytes_per_cell_update": bpc_o,
+                                  "fp64": fp64_roofline(cells, args.flux,
+                                                        "fp32" if other == vah.VAH_FP32 else "fp64",
+                                                        form["avg_stage_ms"] / 1000.0, fp64_peak),
                                   "kernel": "tile_kernel (one TMA-tiled launch per stage)" if other == vah.VAH_FP32
                                   else "one RK stage: face_kernel x3 + cell_kernel"}})
         line["fp32_form" if other == vah.VAH_FP32 else "fp64_form"] = form
