@@ -360,14 +360,13 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             tile_cell_explicit<PHYS, IS3D>(bq, bc, SY, SZ, pr, s, flux, eos, t_src, dt, d.dx, d.dy, d.dz, d.etabar, val,
                                            e_prev, bad);
 
-        // every read of this tile's boxes is done: the next tile's copies
-        // overlap this tile's inversions, regulator and stores
-        if (tid == 0) {
-            s_item = (int)atomicAdd(next_item, 1u);
-            if (s_item < nitems) issue(s_item);
-        }
+        // after this barrier every read of this tile's boxes is done: the
+        // next tile's copies, issued only then, overlap this tile's
+        // inversions, regulator and stores
+        if (tid == 0) s_item = (int)atomicAdd(next_item, 1u);
         __syncthreads();
         const int w_next = s_item;
+        if (tid == 0 && w_next < nitems) issue(w_next);
 
         // ---- the cell: inversion, regulator, stores (stage outputs:
         // FullyDiscreteKurganovTadmorScheme.cpp:761-789) ----
