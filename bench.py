@@ -182,23 +182,25 @@ def event_config(cells=NX * NY * NZ):
 def _ref_worker(args):
     """One worker process: the reference's own CPU step (oracle/_ref, built from
     the reference's sources; the C restatement where it was not built)
-    advancing its own copy of the full 121x121x81 event. The EoS table and the
-    initial condition come from the oracle library's copy of the workload's
-    generators (bit-identical to the library's), so this process maps no
-    product code."""
-    conn, steps, warm, seed = args
+    advancing its block (rows j0..j1, planes k0..k1, all of x) of the
+    121x121x81 event, with the reference's own ghost fill around the block.
+    The EoS table and the initial condition come from the oracle library's
+    copy of the workload's generators (bit-identical to the library's), so
+    this process maps no product code."""
+    conn, steps, warm, seed, (j0, j1, k0, k1) = args
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import vahlib as V
     table = V.oracle_eos_table()
-    g = V.Grid(NX, NY, NZ, DX, DX, DZ, ETA_S, physics="pimunu_pi", eos="table", zeta="crossover", table=table)
+    ny, nz = j1 - j0, k1 - k0
+    g = V.Grid(NX, ny, nz, DX, DX, DZ, ETA_S, physics="pimunu_pi", eos="table", zeta="crossover", table=table)
     use_ref = V.ref_available(g.physics, g.eos)
     impl = V.Reference(g) if use_ref else V.Oracle(g)
     e_peak = V.table_energy_density(table, 0.6 / 0.197326938)
     exy, _ = V.oracle_mc_glauber(NX, NY, DX, DX, B_IMPACT, seed, e_peak=e_peak, e_floor=0.0)
     f = V.oracle_longitudinal(NZ, DZ)
-    e = (f[:, None] * exy[None, :]) + 1e-3
+    e = ((f[:, None] * exy[None, :]) + 1e-3).reshape(NZ, NY, NX)[k0:k1, j0:j1, :]
     full = np.zeros(g.shape)
-    full[2:-2, 2:-2, 2:-2] = e.reshape(NZ, NY, NX)
+    full[2:-2, 2:-2, 2:-2] = e
     n = int(table[0])
     p = np.interp(np.log(np.maximum(full, 1e-300)), table[1] + table[3] * np.arange(n), table[8:8 + n])
     V.load_state(impl, {V.E: full.ravel(), V.PP: p.ravel(), V.UT: np.ones(g.ncell), V.PL: p.ravel()})
@@ -218,14 +220,28 @@ def _ref_worker(args):
     conn.close()
 
 
+def ref_blocks(workers):
+    """The 121x121x81 event cut into at most `workers` blocks of whole x rows:
+    eta slabs of at least 3 planes (3+1D arithmetic in every block), then y
+    bands; the blocks cover every cell once."""
+    def cuts(n, parts):
+        return [round(n * q / parts) for q in range(parts + 1)]
+    pz = max(1, min(workers, NZ // 3))
+    py = max(1, min(workers // pz, NY // 8))
+    kz, jy = cuts(NZ, pz), cuts(NY, py)
+    return [(jy[a], jy[a + 1], kz[b], kz[b + 1]) for b in range(pz) for a in range(py)]
+
+
 def cpu_step_rate(workers, steps, warmup, seed=1):
-    """Spawned workers (one per host core used), each stepping its own copy of
-    the full event in lockstep; returns (cell-updates/s, kind, per-step wall s)."""
+    """One RK2 step of the event per step, its blocks (ref_blocks) stepped in
+    lockstep by spawned workers, one per block and host core; returns
+    (cell-updates/s of the event, kind, per-step wall s)."""
     ctx = mp.get_context("spawn")
     pipes, procs = [], []
-    for w in range(workers):
+    blocks = ref_blocks(workers)
+    for box in blocks:
         a, b = ctx.Pipe()
-        p = ctx.Process(target=_ref_worker, args=((b, steps, warmup, seed),))
+        p = ctx.Process(target=_ref_worker, args=((b, steps, warmup, seed, box),))
         p.start()
         pipes.append(a)
         procs.append(p)
@@ -241,7 +257,7 @@ def cpu_step_rate(workers, steps, warmup, seed=1):
             walls.append(time.perf_counter() - a)
     for p in procs:
         p.join(timeout=60)
-    rate = workers * NX * NY * NZ * len(walls) / sum(walls)
+    rate = NX * NY * NZ * len(walls) / sum(walls)
     return rate, kinds.pop(), walls
 
 
@@ -252,7 +268,7 @@ def host_cores():
         return os.cpu_count() or 1
 
 
-REF_WORKER_BYTES = 1.3e9  # resident size of one reference process on the full event (measured: 1.02 GB)
+REF_EVENT_BYTES = 1.3e9  # resident size of one reference process on the full event (measured: 1.02 GB)
 
 
 def available_memory_bytes():
@@ -285,12 +301,17 @@ def run_reference(args, rank, world):
     cores = host_cores()
     workers = max(1, min(cores, 64))
     mem = available_memory_bytes()
-    if mem is not None:
-        workers = max(1, min(workers, int(0.6 * mem / REF_WORKER_BYTES)))
+    if mem is not None:  # a block's process: the interpreter plus its share of the event's arrays
+        while workers > 1 and len(ref_blocks(workers)) * (0.2e9 + REF_EVENT_BYTES / len(ref_blocks(workers))) > 0.6 * mem:
+            workers -= 1
+    blocks = ref_blocks(workers)
     rate, kind, walls = cpu_step_rate(workers, args.steps, args.warmup)
     ms = 1000 * statistics.mean(walls)
-    sample = (f"the full {NX}x{NY}x{NZ} event (seed 1) in each of {workers} worker processes, one RK2 step per worker "
-              f"per step, in lockstep; {cores} host cores")
+    pz = len({b[2:] for b in blocks})
+    sample = (f"one RK2 step of the {NX}x{NY}x{NZ} event (seed 1) per step, cut into {len(blocks)} blocks "
+              f"({pz} eta slabs x {len(blocks) // pz} y bands, the reference's ghost fill around each) stepped in "
+              f"lockstep by as many worker processes; {cores} host cores")
+    workers = len(blocks)
     line = {"impl": "reference", "metric": "cell-updates/s", "value": rate, "unit": "cell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
