@@ -602,9 +602,11 @@ def run_precision(args, rank, world, dist):
 # measures each of them after the headline (FP64 event) number, with its own
 # clock record, and adds them to the same JSON line.
 
-def event_form_rate(vah, table, e0, precision, steps, warmup, local, stream):
+def event_form_rate(vah, table, e0, precision, steps, warmup, local, stream, e2e_steps=0):
     """One event of the workload in the given form: cell-updates/s over `steps`
-    device-timed steps after `warmup`, with the average stage time."""
+    device-timed steps after `warmup`, with the average stage time; then, when
+    e2e_steps > 0, the same through the host-buffer entry point (pinned FP64
+    host state in and out every step, wall-clocked)."""
     import torch
 
     ev = vah.Event(NX, NY, NZ, DX, DX, DZ, ETA_S, physics=vah.VAH_PIMUNU_PI, eos=vah.VAH_EOS_TABLE,
@@ -626,13 +628,28 @@ def event_form_rate(vah, table, e0, precision, steps, warmup, local, stream):
         torch.cuda.synchronize()
     elapsed = start.elapsed_time(end) / 1000.0
     kms, launches = ev.kernel_time()
+    ev.set_timing(False)
     ev.sync()
     stats = ev.stats()
-    ev.close()
+    t += steps * DT
     cells = NX * NY * NZ
-    return {"value": cells * steps / elapsed, "ms_per_step": 1000 * elapsed / steps,
-            "avg_stage_ms": kms / max(launches, 1), "stage_launches": launches, "clocks": clk.summary(),
-            "fallbacks": {"face": stats.face_fallbacks, "cell": stats.cell_fallbacks, "nan": stats.nan_cells}}
+    out = {"value": cells * steps / elapsed, "ms_per_step": 1000 * elapsed / steps,
+           "avg_stage_ms": kms / max(launches, 1), "stage_launches": launches, "clocks": clk.summary(),
+           "fallbacks": {"face": stats.face_fallbacks, "cell": stats.cell_fallbacks, "nan": stats.nan_cells}}
+    if e2e_steps > 0:
+        host = {fid: torch.from_numpy(ev.get_field(fid)).pin_memory() for fid in range(26)}
+        ptrs = [host[fid].data_ptr() if fid in host else 0 for fid in range(vah.NUM_FIELDS)]
+        ev.step_host(t, DT, ptrs)  # warm
+        t += DT
+        a = time.perf_counter()
+        for n in range(e2e_steps):
+            ev.step_host(t, DT, ptrs)
+            t += DT
+        state_bytes = sum(h.numel() * 8 for h in host.values())
+        out["e2e"] = {"value": cells * e2e_steps / (time.perf_counter() - a), "unit": "cell-updates/s",
+                      "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes, "steps": e2e_steps}
+    ev.close()
+    return out
 
 
 def batch_form_rate(vah, table, precision, nevents, steps, warmup, local, stream):
@@ -784,7 +801,7 @@ def run_vah(args, rank, world, dist):
         line["clocks"] = clk_summary
     if world == 1 and not args.no_extras and args.flux == "per_cell":
         other = vah.VAH_FP32 if prec == vah.VAH_FP64 else vah.VAH_FP64
-        form = event_form_rate(vah, table, e0, other, args.steps, args.warmup, local, stream)
+        form = event_form_rate(vah, table, e0, other, args.steps, args.warmup, local, stream, args.e2e_steps)
         bpc_o = BYTES_PER_CELL_UPDATE // 2 if other == vah.VAH_FP32 else BYTES_PER_CELL_UPDATE
         ach = bpc_o / 2 * cells / (form["avg_stage_ms"] / 1000.0) / 1e9
         form.update({"unit": "cell-updates/s", "dtype": "f32+f64-inversion" if other == vah.VAH_FP32 else "f64",

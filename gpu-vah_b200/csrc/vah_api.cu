@@ -1069,31 +1069,33 @@ extern "C" int vah_event_kernel_time(vah_event *ev, double *ms, long long *launc
 
 namespace {
 
-__global__ void widen_kernel(const float *__restrict__ src, double *__restrict__ dst, size_t n) {
+// FP64 host rows of hx values <-> FP32 device rows of the padded pitch.
+__global__ void widen_kernel(const float *__restrict__ src, double *__restrict__ dst, int hx, int pitch, size_t rows) {
+    const size_t n = (size_t)hx * rows;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-        dst[k] = (double)src[k];
+        dst[k] = (double)src[(k / hx) * pitch + k % hx];
 }
 
-__global__ void narrow_kernel(const double *__restrict__ src, float *__restrict__ dst, size_t n) {
+__global__ void narrow_kernel(const double *__restrict__ src, float *__restrict__ dst, int hx, int pitch, size_t rows) {
+    const size_t n = (size_t)hx * rows;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-        dst[k] = (float)src[k];
+        dst[(k / hx) * pitch + k % hx] = (float)src[k];
 }
 
-// FP32 storage: the caller's FP64 host arrays cross PCIe as FP64 into one
-// field of device staging and are narrowed (widened on the way out) by a
-// kernel, all in stream order, with one synchronisation at the end.
+// FP32 storage: the caller's FP64 host arrays cross PCIe as FP64, one
+// contiguous copy per field into device staging in the host layout, and are
+// narrowed into the padded device rows (widened on the way out) by a kernel,
+// all in stream order, with one synchronisation at the end.
 int step_host_fp32(vah_event *ev, double t, double dt, double *const *fields) {
-    const size_t n = ev->ncell;
-    if (!ev->d_stage64) VAH_TRY(cudaMalloc((void **)&ev->d_stage64, n * sizeof(double)));
-    const int block = 256, grid = (int)std::min<size_t>((n + block - 1) / block, 148 * 16);
-    // host rows of nx + 4 doubles, staging rows of the device pitch
-    const size_t w = (size_t)(ev->lat.nx + 4) * sizeof(double), dp = (size_t)ev->ncx * sizeof(double),
-                 rows = (size_t)ev->ncy * ev->ncz;
+    const int hx = ev->lat.nx + 4;
+    const size_t rows = (size_t)ev->ncy * ev->ncz, hn = (size_t)hx * rows;  // host layout
+    if (!ev->d_stage64) VAH_TRY(cudaMalloc((void **)&ev->d_stage64, ev->ncell * sizeof(double)));
+    const int block = 256, grid = (int)std::min<size_t>((hn + block - 1) / block, 148 * 16);
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {
         float *d = (float *)field_ptr(ev, id);
         if (!d || !fields[id]) continue;
-        VAH_TRY(cudaMemcpy2DAsync(ev->d_stage64, dp, fields[id], w, w, rows, cudaMemcpyHostToDevice, ev->stream));
-        narrow_kernel<<<grid, block, 0, ev->stream>>>(ev->d_stage64, d, n);
+        VAH_TRY(cudaMemcpyAsync(ev->d_stage64, fields[id], hn * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
+        narrow_kernel<<<grid, block, 0, ev->stream>>>(ev->d_stage64, d, hx, ev->ncx, rows);
         VAH_TRY(cudaGetLastError());
     }
     int rc = vah_rk2_step(ev, t, dt);
@@ -1101,9 +1103,9 @@ int step_host_fp32(vah_event *ev, double t, double dt, double *const *fields) {
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {  // pointers after the u <-> up swap
         const float *d = (const float *)field_ptr(ev, id);
         if (!d || !fields[id]) continue;
-        widen_kernel<<<grid, block, 0, ev->stream>>>(d, ev->d_stage64, n);
+        widen_kernel<<<grid, block, 0, ev->stream>>>(d, ev->d_stage64, hx, ev->ncx, rows);
         VAH_TRY(cudaGetLastError());
-        VAH_TRY(cudaMemcpy2DAsync(fields[id], w, ev->d_stage64, dp, w, rows, cudaMemcpyDeviceToHost, ev->stream));
+        VAH_TRY(cudaMemcpyAsync(fields[id], ev->d_stage64, hn * sizeof(double), cudaMemcpyDeviceToHost, ev->stream));
     }
     return vah_event_sync(ev);
 }
