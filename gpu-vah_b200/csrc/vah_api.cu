@@ -156,6 +156,10 @@ vah::Eos make_eos(const vah_event *ev) {
     return eos;
 }
 
+// Whether the steps store the eta ghost layers (3+1D, or validity
+// diagnostics, which read them); else they are filled when read.
+bool zghosts_eager(const vah_event *ev) { return ev->lat.nz > 1 || ev->validity; }
+
 template <typename S>
 void fill_common(const vah_event *ev, StageArgs<S> &a) {
     memset(&a, 0, sizeof(a));
@@ -172,6 +176,7 @@ void fill_common(const vah_event *ev, StageArgs<S> &a) {
     a.dz = ev->lat.dz;
     a.etabar = ev->hydro.eta_over_s;
     a.eos = make_eos(ev);
+    a.zghosts = zghosts_eager(ev);
     a.counters = ev->d_counters;
     for (int d = 0; d < 3; ++d)
         for (int n = 0; n < 16; ++n) {
@@ -275,6 +280,7 @@ int tile_setup(vah_event *ev) {
     d.dt = 0.0;  // events pass their step with each launch
     d.etabar = ev->hydro.eta_over_s;
     d.counters = ev->d_counters;
+    d.zghosts = zghosts_eager(ev);
     VAH_TRY(cudaMalloc((void **)&ev->d_tslot, sizeof(vah::TileSlot)));
     std::vector<vah::TileItem> items;
     vah::tile_items(items, 0, ev->lat.nx, ev->lat.ny, ev->lat.nz);
@@ -600,11 +606,43 @@ extern "C" int vah_event_set_field(vah_event *ev, int field, const double *host,
     return copy_field(ev, d, nullptr, host, with_ghosts);
 }
 
+namespace {
+
+template <typename S>
+int fill_zghosts_t(vah_event *ev, const int *ids, int n) {
+    vah::FieldSet<S> f{};
+    for (int k = 0; k < n; ++k) {
+        // u^{n-1} is a former u buffer once a step has run; before that it is the caller's, which
+        // the reference's ghost fill does not touch (setGhostCellVars, DynamicalVariables.cpp:358-389)
+        void *d = ids[k] >= VAH_F_UPT && ev->steps == 0 ? nullptr : field_ptr(ev, ids[k]);
+        if (d) f.f[f.n++] = (S *)d;
+        if (f.n == 32 || (k == n - 1 && f.n)) {
+            VAH_TRY(vah::launch_ghost_pass<S>(f, ev->lat.nx, ev->lat.ny, ev->lat.nz, ev->ncx, 2, ev->stream));
+            f.n = 0;
+        }
+    }
+    return VAH_OK;
+}
+
+// 2+1D events whose steps leave the eta ghost layers (no stencil reads them):
+// the eta pass of the reference's ghost fill (setGhostCellsKernelK) over the
+// given fields, before a caller reads them with ghosts. Stream-ordered.
+int fill_zghosts(vah_event *ev, const int *ids, int n) {
+    if (zghosts_eager(ev) || n <= 0) return VAH_OK;
+    return ev->elem == sizeof(float) ? fill_zghosts_t<float>(ev, ids, n) : fill_zghosts_t<double>(ev, ids, n);
+}
+
+}  // namespace
+
 extern "C" int vah_event_get_field(vah_event *ev, int field, double *host, int with_ghosts) {
     if (!ev || !host) return VAH_ERR_ARG;
     void *d = field_ptr(ev, field);
     if (!d) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(ev->opt.device));
+    if (with_ghosts) {
+        const int rc = fill_zghosts(ev, &field, 1);
+        if (rc != VAH_OK) return rc;
+    }
     return copy_field(ev, d, host, nullptr, with_ghosts);
 }
 
@@ -945,9 +983,16 @@ extern "C" int vah_event_set_validity(vah_event *ev, int on) {
             if (e != cudaSuccess) return cuda_status(e);
         }
     }
+    if (on && !ev->validity && ev->lat.nz == 1) {  // the diagnostics read the eta ghost layers: fill them now
+        int ids[VAH_NUM_FIELDS];
+        for (int id = 0; id < VAH_NUM_FIELDS; ++id) ids[id] = id;
+        const int rc = fill_zghosts(ev, ids, VAH_NUM_FIELDS);
+        if (rc != VAH_OK) return rc;
+    }
     ev->validity = on != 0;
     if (ev->tile) {  // the tile kernel writes the regulator maps through its descriptor
         for (int m = 0; m < 11; ++m) ev->h_tslot.regmap[m] = ev->validity ? ev->vd[VAH_V_REGULATIONS + m] : nullptr;
+        ev->h_tslot.zghosts = zghosts_eager(ev);
         return tile_sync_desc(ev);
     }
     return VAH_OK;
@@ -1069,6 +1114,14 @@ extern "C" int vah_event_kernel_time(vah_event *ev, double *ms, long long *launc
 
 namespace {
 
+// The eta ghost layers of the fields a host-buffer step returns (2+1D).
+int fill_host_zghosts(vah_event *ev, double *const *fields) {
+    int ids[VAH_NUM_FIELDS], n = 0;
+    for (int id = 0; id < VAH_NUM_FIELDS; ++id)
+        if (fields[id]) ids[n++] = id;
+    return fill_zghosts(ev, ids, n);
+}
+
 // FP64 host rows of hx values <-> FP32 device rows of the padded pitch.
 __global__ void widen_kernel(const float *__restrict__ src, double *__restrict__ dst, int hx, int pitch, size_t rows) {
     const size_t n = (size_t)hx * rows;
@@ -1100,6 +1153,7 @@ int step_host_fp32(vah_event *ev, double t, double dt, double *const *fields) {
     }
     int rc = vah_rk2_step(ev, t, dt);
     if (rc != VAH_OK) return rc;
+    if ((rc = fill_host_zghosts(ev, fields)) != VAH_OK) return rc;
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {  // pointers after the u <-> up swap
         const float *d = (const float *)field_ptr(ev, id);
         if (!d || !fields[id]) continue;
@@ -1241,6 +1295,7 @@ extern "C" int vah_rk2_step_host(vah_event *ev, double t, double dt, double *con
     }
     rc = vah_rk2_step(ev, t, dt);
     if (rc != VAH_OK) return rc;
+    if ((rc = fill_host_zghosts(ev, fields)) != VAH_OK) return rc;
     for (int id = 0; id < VAH_NUM_FIELDS; ++id) {  // pointers after the u <-> up swap
         void *d = field_ptr(ev, id);
         if (d && fields[id]) VAH_TRY(cudaMemcpyAsync(fields[id], d, bytes, cudaMemcpyDeviceToHost, ev->stream));

@@ -84,6 +84,7 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
     a.t_src = stage == 1 ? c.t : c.t + d.dt;
     a.t_inv = c.t + d.dt;
     a.stage2 = stage == 2;
+    a.zghosts = d.nz > 1;  // 2+1D: the eta ghost layers are filled when a caller reads them
     a.eos = eos;
     a.counters = d.counters;
     a.fallback = d.fallback;
@@ -544,6 +545,7 @@ int fill_slot(vah_batch *b, int slot) {
         t.dt = d.dt;
         t.etabar = d.etabar;
         t.counters = d.counters;
+        t.zghosts = d.nz > 1;      // 2+1D: the eta ghost layers are filled when a caller reads them
         t.fallback2 = d.fallback;  // the batch keeps the latest (stage-2) flags
         t.hot = d.hot;
         t.e_freeze = d.e_freeze;
@@ -1064,6 +1066,19 @@ extern "C" int vah_batch_get_field(vah_batch *b, int slot, int field, double *ho
     const size_t es = b->elem;
     if (es == sizeof(float)) f32.resize(n);
     void *dst = es == sizeof(float) ? (void *)f32.data() : (void *)host;
+    if (with_ghosts && lat.nz == 1) {  // 2+1D steps leave the eta ghost layers to the reader
+        if (es == sizeof(float)) {
+            vah::FieldSet<float> f{};
+            f.f[0] = (float *)src;
+            f.n = 1;
+            VAH_TRY(vah::launch_ghost_pass<float>(f, lat.nx, lat.ny, lat.nz, (int)ncx, 2, b->stream));
+        } else {
+            vah::FieldSet<double> f{};
+            f.f[0] = (double *)src;
+            f.n = 1;
+            VAH_TRY(vah::launch_ghost_pass<double>(f, lat.nx, lat.ny, lat.nz, (int)ncx, 2, b->stream));
+        }
+    }
     if (with_ghosts) {
         VAH_TRY(cudaMemcpy2DAsync(dst, hx * es, src, ncx * es, hx * es, ncy * (lat.nz + 4), cudaMemcpyDeviceToHost,
                                   b->stream));

@@ -104,5 +104,10 @@ cudaError_t launch_init_primitives(const FieldSet<S> &q, const FieldSet<S> &u, c
 // Reference ghost fill, three passes with its loop ranges (setGhostCells).
 template <typename S>
 cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, int pitch, cudaStream_t stream);
+// One pass of it (0: x, 1: y, 2: eta): on 2+1D lattices the eta pass fills the
+// eta ghost layers that the steps leave to the reader.
+template <typename S>
+cudaError_t launch_ghost_pass(const FieldSet<S> &fields, int nx, int ny, int nz, int pitch, int pass,
+                              cudaStream_t stream);
 
 }  // namespace vah

@@ -300,6 +300,17 @@ cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, int
     return cudaSuccess;
 }
 
+// One pass of the ghost fill (0: x, 1: y, 2: eta), as launch_ghosts runs it.
+template <typename S>
+cudaError_t launch_ghost_pass(const FieldSet<S> &fields, int nx, int ny, int nz, int pitch, int pass,
+                              cudaStream_t stream) {
+    const int block = 256;
+    long long n = pass == 0 ? (long long)ny * nz : (pass == 1 ? (long long)nx * nz : (long long)nx * ny);
+    n = (n + 4LL * (nx + ny + nz) + 16) * 4;
+    ghost_kernel<S><<<grid_for(n, block), block, 0, stream>>>(fields, nx, ny, nz, pitch, pass);
+    return cudaGetLastError();
+}
+
 #define VAH_INSTANTIATE(S)                                                                                      \
     template cudaError_t launch_stage<S>(const StageArgs<S> &, int, cudaStream_t);                              \
     template cudaError_t launch_validity<S>(const ValidityArgs<S> &, int, cudaStream_t);                        \
@@ -312,6 +323,7 @@ cudaError_t launch_ghosts(const FieldSet<S> &fields, int nx, int ny, int nz, int
                                                  const S *, int, int, int, int, int, double, int, cudaStream_t); \
     template cudaError_t launch_init_primitives<S>(const FieldSet<S> &, const FieldSet<S> &, const S *, S *,    \
                                                    const Eos &, int, int, int, int, cudaStream_t);             \
-    template cudaError_t launch_ghosts<S>(const FieldSet<S> &, int, int, int, int, cudaStream_t);
+    template cudaError_t launch_ghosts<S>(const FieldSet<S> &, int, int, int, int, cudaStream_t);              \
+    template cudaError_t launch_ghost_pass<S>(const FieldSet<S> &, int, int, int, int, int, cudaStream_t);
 
 }  // namespace vah

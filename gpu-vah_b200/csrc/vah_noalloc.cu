@@ -142,6 +142,7 @@ extern "C" int vah_stage_noalloc(const vah_lattice *lat, double eta_over_s, int 
     a.t_src = stage == 1 ? t : t + dt;
     a.t_inv = t + dt;
     a.stage2 = stage == 2;
+    a.zghosts = 1;  // the caller's buffers come back with every ghost layer a stage writes
     a.eos.kind = eos == VAH_EOS_TABLE ? 1 : 0;
     a.eos.zeta = zeta == VAH_ZETA_CROSSOVER ? 1 : 0;
     a.eos.tab = d_eos_table;

@@ -30,6 +30,9 @@ struct StageArgs {
     double dt, dx, dy, dz, etabar;
     int stage2;       // 1: convex combination with qavg before inversion
     int shared_faces; // unused by the per-cell path
+    int zghosts;      // 1: boundary cells also store the eta ghost layers. On 2+1D lattices no stencil
+                      // reads them, so the event and batch paths leave them to a fill when a caller reads
+                      // fields with ghosts (and keep them when validity diagnostics, which read them, run)
     const S *qin[16];
     const S *uin[4];
     const S *upin[4];   // previous-stage velocity (centre only)
@@ -233,8 +236,10 @@ VAH_HD void stage_cell(const StageArgs<S> &a, int i, int j, int k) {
     if (i == a.nx + 1) { store_cell(a, s + 1, NQ, val, u, e, p); store_cell(a, s + 2, NQ, val, u, e, p); }
     if (j == 2) { store_cell(a, s - sy, NQ, val, u, e, p); store_cell(a, s - 2 * sy, NQ, val, u, e, p); }
     if (j == a.ny + 1) { store_cell(a, s + sy, NQ, val, u, e, p); store_cell(a, s + 2 * sy, NQ, val, u, e, p); }
-    if (k == 2) { store_cell(a, s - sz, NQ, val, u, e, p); store_cell(a, s - 2 * sz, NQ, val, u, e, p); }
-    if (k == a.nz + 1) { store_cell(a, s + sz, NQ, val, u, e, p); store_cell(a, s + 2 * sz, NQ, val, u, e, p); }
+    if (a.zghosts) {
+        if (k == 2) { store_cell(a, s - sz, NQ, val, u, e, p); store_cell(a, s - 2 * sz, NQ, val, u, e, p); }
+        if (k == a.nz + 1) { store_cell(a, s + sz, NQ, val, u, e, p); store_cell(a, s + 2 * sz, NQ, val, u, e, p); }
+    }
 }
 
 // ------------------------------------------------------- face/cell split --
@@ -353,8 +358,10 @@ VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
     if (i == a.nx + 1) { store_cell(a, s + 1, NQ, val, u, e, p); store_cell(a, s + 2, NQ, val, u, e, p); }
     if (j == 2) { store_cell(a, s - sy, NQ, val, u, e, p); store_cell(a, s - 2 * sy, NQ, val, u, e, p); }
     if (j == a.ny + 1) { store_cell(a, s + sy, NQ, val, u, e, p); store_cell(a, s + 2 * sy, NQ, val, u, e, p); }
-    if (k == 2) { store_cell(a, s - sz, NQ, val, u, e, p); store_cell(a, s - 2 * sz, NQ, val, u, e, p); }
-    if (k == a.nz + 1) { store_cell(a, s + sz, NQ, val, u, e, p); store_cell(a, s + 2 * sz, NQ, val, u, e, p); }
+    if (a.zghosts) {
+        if (k == 2) { store_cell(a, s - sz, NQ, val, u, e, p); store_cell(a, s - 2 * sz, NQ, val, u, e, p); }
+        if (k == a.nz + 1) { store_cell(a, s + sz, NQ, val, u, e, p); store_cell(a, s + 2 * sz, NQ, val, u, e, p); }
+    }
 }
 
 // ------------------------------------------------------------ set-up ops --

@@ -73,6 +73,7 @@ struct alignas(64) TileSlot {
     float *uA[4], *uB[4], *uS[4];
     long long fstride;
     int nx, ny, nz, pitch, ncy, nq;
+    int zghosts;                   // 2+1D: 1 to store the eta ghost layers (else filled when read)
     double dx, dy, dz, dt, etabar;
     unsigned long long *counters;  // [face fallbacks, cell fallbacks, NaN cells]
     unsigned char *fallback1, *fallback2;  // optional: per cell, 1 where the stage-1 / stage-2 inversion fell back
@@ -413,8 +414,10 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             if (ci == d.nx - 1) { store(s + 1); store(s + 2); }
             if (cj == 0) { store(s - sy); store(s - 2 * sy); }
             if (cj == d.ny - 1) { store(s + sy); store(s + 2 * sy); }
-            if (ck == 0) { store(s - sz); store(s - 2 * sz); }
-            if (ck == d.nz - 1) { store(s + sz); store(s + 2 * sz); }
+            if (IS3D || d.zghosts) {
+                if (ck == 0) { store(s - sz); store(s - 2 * sz); }
+                if (ck == d.nz - 1) { store(s + sz); store(s + 2 * sz); }
+            }
         }
         w = w_next;
     }

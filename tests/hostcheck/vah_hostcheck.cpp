@@ -87,6 +87,7 @@ void common(HostEvent *h, vah::StageArgs<double> &a) {
     a.plane = (long long)h->ncx * h->ncy;
     a.dx = h->dx; a.dy = h->dy; a.dz = h->dz; a.etabar = h->etabar;
     a.eos = h->eos;
+    a.zghosts = 1;  // every ghost layer the stage writes, as the oracle's arrays hold them
     a.counters = h->counters;
     for (int d = 0; d < 3; ++d)
         for (int n = 0; n < 16; ++n) {
