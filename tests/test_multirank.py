@@ -55,3 +55,22 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
         steps, warmup, gpus = 1, 0, 2
     bench.run_reference(Args, 1, 2)
     assert calls == []
+
+
+def test_reference_arm_blocks_cover_the_event_once():
+    """The reference arm's per-step sample is the whole 121x121x81 event, cut
+    into blocks of whole x rows: every cell in exactly one block, each block
+    at least 3 eta planes deep (3+1D arithmetic), at most one block per
+    worker."""
+    import numpy as np
+
+    import bench
+
+    for workers in (1, 2, 7, 16, 27, 40, 64, 200):
+        blocks = bench.ref_blocks(workers)
+        assert 1 <= len(blocks) <= workers
+        hits = np.zeros((bench.NZ, bench.NY), int)
+        for j0, j1, k0, k1 in blocks:
+            assert k1 - k0 >= 3 and j1 > j0
+            hits[k0:k1, j0:j1] += 1
+        assert np.all(hits == 1), workers
