@@ -652,6 +652,44 @@ def event_form_rate(vah, table, e0, precision, steps, warmup, local, stream, e2e
     return out
 
 
+def late_regime_rates(vah, table, e0, precision, local, stream, steps=20):
+    """The same event later in its evolution: device-timed `steps` steps from
+    tau = 1.0 fm/c (flow developed, no inversion fallback yet) and from
+    tau = 1.4 fm/c (the reference's inversion fallback spreading through the
+    dilute edge; the event reaches NaN soon after 1.5), with the fallbacks per
+    step in each window; a window that meets a NaN says so instead."""
+    import torch
+
+    ev = vah.Event(NX, NY, NZ, DX, DX, DZ, ETA_S, physics=vah.VAH_PIMUNU_PI, eos=vah.VAH_EOS_TABLE,
+                   zeta=vah.VAH_ZETA_CROSSOVER, table=table, t0=T0, device=local, stream=stream.cuda_stream,
+                   precision=precision)
+    ev.init_from_e(T0, e0, vah.VAH_PL_REFERENCE)
+    t, out = T0, {}
+    for start in (1.0, 1.4):
+        n = int(round((start - t) / DT))
+        ev.run(t, DT, n)
+        t += n * DT
+        s0 = ev.stats()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ev.run(t, DT, steps)
+        b.record(stream)
+        torch.cuda.synchronize()
+        t += steps * DT
+        s1 = ev.stats()
+        key = f"tau_{start:.1f}"
+        if s1.nan_cells:
+            out[key] = {"nan_cells": s1.nan_cells}
+            break
+        ms = a.elapsed_time(b) / steps
+        out[key] = {"ms_per_step": ms, "value": NX * NY * NZ / (ms / 1000.0),
+                    "face_fallbacks_per_step": (s1.face_fallbacks - s0.face_fallbacks) / steps,
+                    "cell_fallbacks_per_step": (s1.cell_fallbacks - s0.cell_fallbacks) / steps}
+    ev.close()
+    return out
+
+
 def batch_form_rate(vah, table, precision, nevents, steps, warmup, local, stream):
     """The 2+1D batch workload (nevents MC-Glauber events, sides from
     {81, 121, 161, 201}, b uniform in [0, 12] fm, dx = 0.1 fm, initial
@@ -816,6 +854,8 @@ def run_vah(args, rank, world, dist):
                                   "kernel": "tile_kernel (one TMA-tiled launch per stage)" if other == vah.VAH_FP32
                                   else "one RK stage: face_kernel x3 + cell_kernel"}})
         line["fp32_form" if other == vah.VAH_FP32 else "fp64_form"] = form
+        line["late"] = {name: late_regime_rates(vah, table, e0, p, local, stream)
+                        for name, p in (("fp64", vah.VAH_FP64), ("fp32", vah.VAH_FP32))}
         line["batch"] = {name: batch_form_rate(vah, table, p, 256, args.steps, args.warmup, local, stream)
                          for name, p in (("fp64", vah.VAH_FP64), ("fp32", vah.VAH_FP32))}
         line["batch"]["workload"] = ("256 2+1D MC-Glauber events, sides {81,121,161,201}, dx=0.1, b~U[0,12] fm, "
