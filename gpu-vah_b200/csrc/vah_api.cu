@@ -718,6 +718,8 @@ int init_device_ic(vah_event *ev, double t0, const vah_glauber *g, const vah_opt
     const int A = g ? g->A : o->A;
     const double eta_flat = g ? g->eta_flat : o->eta_flat, sigma_eta = g ? g->sigma_eta : o->sigma_eta;
     if (A < 1 || (lat.nz > 1 && !(sigma_eta > 0))) return VAH_ERR_ARG;
+    const double R = g ? g->ws_R : o->ws_R, a = g ? g->ws_a : o->ws_a;
+    if (!(R > 0) || !(a > 0) || !std::isfinite(R + a)) return VAH_ERR_ARG;
     if (g && (A > 256 || !(g->width > 0))) return VAH_ERR_ARG;
     if (o && !(o->sigma_nn_fm2 > 0)) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(ev->opt.device));
@@ -737,6 +739,13 @@ int init_device_ic(vah_event *ev, double t0, const vah_glauber *g, const vah_opt
     } else if (err == cudaSuccess) {
         err = vah::ic_optical_device(lat.nx, lat.ny, lat.dx, lat.dy, o->b, o->sigma_nn_fm2, A, o->ws_R, o->ws_a,
                                      o->x_coll, d_aux, d_v, maxbits, ev->stream);
+    }
+    int np = 0;  // the sampler reports -1 when its draws ran out (parameters it cannot sample)
+    if (err == cudaSuccess && g) err = cudaMemcpyAsync(&np, scratch + 64, sizeof(int), cudaMemcpyDeviceToHost, ev->stream);
+    if (err == cudaSuccess && g) err = cudaStreamSynchronize(ev->stream);
+    if (err == cudaSuccess && np < 0) {
+        VAH_TRY(cudaFreeAsync(scratch, ev->stream));
+        return VAH_ERR_ARG;
     }
     const double e_peak = g ? g->e_peak : o->e_peak, e_floor = g ? g->e_floor : o->e_floor;
     if (err == cudaSuccess)

@@ -721,7 +721,9 @@ vah::FieldSet<S> fs(S *const *p, int n) {
 // GPU; scratch from the batch's pool, freed in stream order.
 template <typename S>
 int glauber_slot(vah_batch *b, const SlotDesc<S> &d, const vah_lattice &lat, const vah_glauber &g) {
-    if (g.A < 1 || g.A > 256 || !(g.width > 0) || (lat.nz > 1 && !(g.sigma_eta > 0))) return VAH_ERR_ARG;
+    if (g.A < 1 || g.A > 256 || !(g.width > 0) || !(g.ws_R > 0) || !(g.ws_a > 0) || !std::isfinite(g.ws_R + g.ws_a) ||
+        (lat.nz > 1 && !(g.sigma_eta > 0)))
+        return VAH_ERR_ARG;
     const size_t nxy = (size_t)lat.nx * lat.ny;
     const size_t bytes = 256 + sizeof(double) * (4 * (size_t)g.A + nxy);
     char *scratch = nullptr;
@@ -732,6 +734,13 @@ int glauber_slot(vah_batch *b, const SlotDesc<S> &d, const vah_lattice &lat, con
     VAH_TRY(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), b->stream));
     VAH_TRY(vah::ic_participants_device(g.b, g.sigma_nn_fm2, g.A, g.ws_R, g.ws_a, g.seed, d_pxy, d_np, b->stream));
     VAH_TRY(vah::ic_deposit_device(d_pxy, d_np, g.width, lat.nx, lat.ny, lat.dx, lat.dy, d_v, maxbits, b->stream));
+    int np = 0;  // the sampler reports -1 when its draws ran out (parameters it cannot sample)
+    VAH_TRY(cudaMemcpyAsync(&np, d_np, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    VAH_TRY(cudaStreamSynchronize(b->stream));
+    if (np < 0) {
+        VAH_TRY(cudaFreeAsync(scratch, b->stream));
+        return VAH_ERR_ARG;
+    }
     VAH_TRY(vah::ic_fill_device<S>(d_v, maxbits, lat.nx, lat.ny, lat.nz, d.ncx, lat.dz, g.eta_flat, g.sigma_eta,
                                    g.e_peak, g.e_floor, d.ep[0][0], b->stream));
     VAH_TRY(cudaFreeAsync(scratch, b->stream));

@@ -10,7 +10,8 @@ namespace vah {
 
 namespace {
 
-constexpr int kMaxA = 256;  // nucleons per nucleus the sampling block holds
+constexpr int kMaxA = 256;           // nucleons per nucleus the sampling block holds
+constexpr long long kMaxDraws = 1 << 22;  // rejection-sampling draws per nucleus before the sampler gives up
 
 // splitmix64, as the host generator (vah_ic.cpp)
 __device__ __forceinline__ uint64_t sm_next(uint64_t &s) {
@@ -26,21 +27,32 @@ __device__ __forceinline__ double sm_uniform(uint64_t &s) { return (sm_next(s) >
 // sampling of r^2 rho(r) on [0, R + 10 a], isotropic directions, shifted by
 // +-b/2 along x), then every thread flags nucleons with a partner of the
 // other nucleus within sqrt(sigma_NN / pi), and a scan writes the
-// participants in order (A's, then B's).
+// participants in order (A's, then B's). A nucleus that needs more than
+// kMaxDraws draws in all (Au with R = 6.38, a = 0.535 fm takes about 4,000)
+// stops the sampler within a fraction of a second: *np = -1.
 __global__ void __launch_bounds__(512) participants_kernel(double b, double sigma, int A, double R, double a,
                                                            unsigned long long seed, double *pxy, int *np) {
     __shared__ double x[2][kMaxA], y[2][kMaxA];
     __shared__ int flag[2 * kMaxA], pos[2 * kMaxA];
+    __shared__ int failed;
     const int tid = threadIdx.x;
+    if (tid == 0) failed = 0;
+    __syncthreads();
     if (tid < 2) {
         uint64_t s = seed * 2 + (unsigned long long)tid + 0x1234567ull;
         const double rmax = R + 10 * a, shift = tid == 0 ? +b / 2 : -b / 2;
+        long long draws = 0;
         for (int n = 0; n < A; ++n) {
-            double r;
-            for (;;) {
+            double r = 0.0;
+            bool hit = false;
+            for (; draws < kMaxDraws && !hit; ++draws) {
                 r = rmax * sm_uniform(s);
                 const double f = (r * r / (rmax * rmax)) / (1 + exp((r - R) / a));
-                if (sm_uniform(s) < f) break;
+                hit = sm_uniform(s) < f;
+            }
+            if (!hit) {
+                atomicExch(&failed, 1);
+                break;
             }
             const double cth = 2 * sm_uniform(s) - 1, phi = 2 * M_PI * sm_uniform(s);
             const double sth = sqrt(1 - cth * cth);
@@ -49,6 +61,10 @@ __global__ void __launch_bounds__(512) participants_kernel(double b, double sigm
         }
     }
     __syncthreads();
+    if (failed) {
+        if (tid == 0) *np = -1;
+        return;
+    }
     const double d2max = sigma / M_PI;
     for (int k = tid; k < 2 * A; k += blockDim.x) {
         const int nu = k < A ? 0 : 1, m = k < A ? k : k - A;
@@ -177,7 +193,8 @@ int grid_of(long long n, int block) {
 
 cudaError_t ic_participants_device(double b, double sigma_nn_fm2, int A, double ws_R, double ws_a,
                                    unsigned long long seed, double *d_pxy, int *d_np, cudaStream_t stream) {
-    if (A < 1 || A > kMaxA) return cudaErrorInvalidValue;
+    if (A < 1 || A > kMaxA || !(ws_R > 0) || !(ws_a > 0) || !std::isfinite(ws_R + ws_a + b + sigma_nn_fm2))
+        return cudaErrorInvalidValue;
     participants_kernel<<<1, 512, 0, stream>>>(b, sigma_nn_fm2, A, ws_R, ws_a, seed, d_pxy, d_np);
     return cudaGetLastError();
 }

@@ -317,7 +317,9 @@ int vah_batch_remove(vah_batch *b, int slot);
  * a grid deposits their Gaussians), e(x, y, eta) = e_peak v(x,y) / max v *
  * f(eta) + e_floor with f vah_ic_longitudinal's profile (1 in 2+1D); then as
  * vah_batch_add. Positions and e agree with the host generator to rounding
- * (the GPU's exp, sin, cos). A <= 256; VAH_ERR_ARG otherwise. */
+ * (the GPU's exp, sin, cos). VAH_ERR_ARG unless 1 <= A <= 256, ws_R > 0, ws_a > 0
+ * (finite) and width > 0; also when the rejection sampler runs out of draws
+ * (4 million per nucleus, for parameters it cannot sample). */
 typedef struct vah_glauber {
     double b, sigma_nn_fm2;
     int A;

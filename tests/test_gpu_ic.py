@@ -88,6 +88,10 @@ def test_device_initial_conditions_reject_bad_arguments():
     assert L.vah_event_init_glauber(ev.ev, 0.5, C.byref(gl), 1) == -1
     gl.sigma_eta, gl.width = 1.3, 0.0
     assert L.vah_event_init_glauber(ev.ev, 0.5, C.byref(gl), 1) == -1
+    gl.width, gl.ws_a = 0.5, 0.0  # no Woods-Saxon surface thickness
+    assert L.vah_event_init_glauber(ev.ev, 0.5, C.byref(gl), 1) == -1
+    gl.ws_a, gl.ws_R = 0.535, float("inf")
+    assert L.vah_event_init_glauber(ev.ev, 0.5, C.byref(gl), 1) == -1
     op = vah.Optical(6.0, 0.0, 197, 6.38, 0.535, 0.15, 5.0, 0.01, 1.5, 1.3)  # sigma_NN = 0
     L.vah_event_init_optical_glauber.argtypes = [C.c_void_p, C.c_double, C.POINTER(vah.Optical), C.c_int]
     assert L.vah_event_init_optical_glauber(ev.ev, 0.5, C.byref(op), 1) == -1
