@@ -146,7 +146,10 @@ int vah_event_destroy(vah_event *ev);
 
 /* Copy one field between host memory and the event (reference layout;
  * with_ghosts = 1: full nc* array, 0: interior nx*ny*nz only). Replaces the
- * host<->device copies of DynamicalVariables.cu:394-482. */
+ * host<->device copies of DynamicalVariables.cu:394-482. On 2+1D lattices the
+ * steps leave the eta ghost layers (no stencil reads them); a read with
+ * ghosts first fills them with the eta pass of the reference's ghost fill
+ * (setGhostCellsKernelK), as vah_batch_get_field and vah_rk2_step_host do. */
 int vah_event_set_field(vah_event *ev, int field, const double *host, int with_ghosts);
 int vah_event_get_field(vah_event *ev, int field, double *host, int with_ghosts);
 
