@@ -43,6 +43,45 @@ def test_gpu_validity_matches_oracle(case, flux):
     ev.close()
 
 
+@pytest.mark.parametrize("case", ["conformal_2d", "table_3d_bulk"])
+def test_gpu_validity_of_the_fp32_form_tracks_the_fp64_form(case):
+    """The FP32 form (tile kernel, FP32 state) fills the same diagnostics: after
+    6 steps, against the FP64 form (FP32 state and shared faces against FP64
+    and reference faces), normwise: the Knudsen numbers, first-order inverse
+    Reynolds numbers, tau_pi and the shear combinations within 1e-3; the
+    regulator's factors, which the FP32 form computes in FP32, within 1e-2.
+    The second-order inverse Reynolds numbers divide by sigma_T:sigma_T, which
+    vanishes where the flow is still boost invariant, so they are compared
+    cell by cell: at least 95% of the cells within 1e-2 (measured: all but 1.2%
+    of the 3+1D slab's cells, those where the transverse shear nearly
+    vanishes; the ratio there is set by rounding in either form)."""
+    if case == "conformal_2d":
+        g, e, t0, dt = (*conformal_workload(31, 29), 0.5, 0.02)
+    else:
+        g, e, t0, dt = table_slab()
+    evs = []
+    for prec in (0, 1):
+        ev = V.Event(g, t0=t0, precision=prec)
+        ev.init_from_e(t0, e, 1)
+        ev.set_validity(1)
+        ev.run(t0, dt, 6)
+        ev.sync()
+        evs.append(ev)
+    errs = validity_errors(g, evs[0].get_validity, evs[1].get_validity)
+    second_order = (V.V_RPI2, V.V_RPI2_BULK)
+    for vid, err in enumerate(errs):
+        if vid in second_order:
+            a, b = g.interior(evs[1].get_validity(vid)), g.interior(evs[0].get_validity(vid))
+            rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+            frac = float(np.mean(rel > 1e-2)) if b.any() else 0.0
+            print(case, vid, f"cells beyond 1e-2: {frac:.2e} (normwise {err:.2e})")
+            assert frac < 5e-2, (vid, frac)
+        else:
+            assert err < (1e-2 if vid >= V.V_REGULATIONS else 1e-3), (vid, err)
+    for ev in evs:
+        ev.close()
+
+
 def test_gpu_validity_leaves_the_evolution_unchanged():
     g, e, t0, dt = table_slab()
     states = []

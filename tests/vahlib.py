@@ -198,6 +198,7 @@ class Oracle:
 REF_VALIDITY_MEMBER = [0, 1, 2, 3, 4, 5, 7, 8, 26, 27, 28, 29, 22, 23, 24, 25, 11, 12, 13, 14, 15, 16, 17, 18, 19,
                        20, 21]
 NUM_VALIDITY = 27
+V_RPI2, V_RPI2_BULK, V_REGULATIONS = 6, 7, 16  # VAH_V_RPI2, VAH_V_RPI2_BULK, VAH_V_REGULATIONS
 
 
 def ref_path(physics, eos):
