@@ -278,8 +278,10 @@ extern "C" int vah_run_plugin(void *latticeParams, void *initCondParams, void *h
 
     vah_lattice vl{nx, ny, nz, dx, dy, dz};
     vah_hydro vh{t0, hydro->shearViscosityToEntropyDensity, hydro->freezeoutTemperatureGeV};
+    static const char *precision_names[] = {"fp64", "fp32"};  // the FP64 form (default) or the FP32 form
+    const int precision = env_choice("VAH_PRECISION", precision_names, 2, VAH_FP64);
     vah_options vo{physics, eos.kind, eos.kind == VAH_EOS_TABLE ? VAH_ZETA_CROSSOVER : VAH_ZETA_REFERENCE,
-                   VAH_FP64, VAH_FLUX_PER_CELL, device, nullptr};
+                   precision, VAH_FLUX_PER_CELL, device, nullptr};
     vah_event *ev = nullptr;
     int rc = vah_event_create(&vl, &vh, &vo, eos.kind == VAH_EOS_TABLE ? eos.tab.data() : nullptr, &ev);
     if (rc != VAH_OK) return rc;

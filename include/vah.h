@@ -49,7 +49,8 @@ extern "C" {
 
 /* ---- storage precision ---- */
 #define VAH_FP64 0 /* state stored and updated in FP64 */
-#define VAH_FP32 1 /* state stored in FP32; inversion and reductions in FP64 */
+#define VAH_FP32 1 /* state, reconstruction, flux and sources in FP32; Newton inversions, closure fits and
+                     reductions in FP64; one TMA-tiled launch per RK stage */
 
 /* ---- face-flux evaluation ---- */
 #define VAH_FLUX_PER_CELL 0       /* each face evaluated by both neighbouring cells with that cell's

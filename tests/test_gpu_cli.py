@@ -70,3 +70,28 @@ def test_gpu_vah_executable_matches_oracle(tmp_path):
         for vid in (0, 2, 4, 6, 16):  # Knudsen numbers, Rpi, Rpi2, the regulator's factor
             name = V.product.VALIDITY_NAMES[vid]
             assert close(dat(str(out), name, t), g.interior(o.validity(vid)).ravel(), rel=1e-6), (name, t)
+
+
+def test_gpu_vah_executable_runs_the_fp32_form(tmp_path):
+    """VAH_PRECISION=fp32 runs the same program in the FP32 form: its outputs
+    track the oracle's FP64 evolution within 1e-4 (normwise) after 20 steps."""
+    cfg, out = tmp_path / "conf", tmp_path / "out"
+    cfg.mkdir()
+    out.mkdir()
+    write_config(str(cfg))
+    env = dict(os.environ, VAH_PHYSICS="pimunu", VAH_EOS="conformal", VAH_PRECISION="fp32")
+    run = subprocess.run([EXE, "-c", str(cfg), "-o", str(out), "-h"], capture_output=True, text=True, env=env,
+                         timeout=300)
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr[-2000:]
+    g = V.Grid(NX, NY, 1, 0.2, 0.2, 0.2, 0.2, physics="pimunu", eos="conformal")
+    e0 = dat(str(out), "e", T0)
+    full = np.zeros(g.shape)
+    full[2:-2, 2:-2, 2:-2] = e0.reshape(1, NY, NX)
+    o = V.Oracle(g)
+    V.load_state(o, {V.E: full.ravel(), V.PP: full.ravel() / 3, V.UT: np.ones(g.ncell)})
+    o.set_conserved(T0, 0)
+    o.set_ghost_cells()
+    o.run(T0, DT, 20)
+    t = T0 + 20 * DT
+    for fid, name in ((V.E, "e"), (V.PL, "pl"), (V.UT, "ut"), (V.UX, "ux"), (V.UY, "uy")):
+        assert close(dat(str(out), name, t), g.interior(o.field(fid)).ravel(), rel=1e-4, absolute=1e-7), name
