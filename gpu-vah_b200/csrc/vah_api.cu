@@ -51,7 +51,8 @@ struct vah_event {
     unsigned char *d_fb;             // optional: per ghosted cell, stage-1 then stage-2 inversion fallback flags
     long long steps;
     double last_t, last_dt;          // time and step of the latest vah_rk2_step (autotuning state)
-    double *d_stage64;               // FP32 storage: one FP64 field of staging for the host-buffer step
+    double *d_stage64;               // FP32 storage: one FP64 field of staging for the host-buffer step ...
+    double *d_stage_all;             // ... and every field, host layout, for its overlapped form (3+1D)
     bool validity;                   // fill the validity diagnostics every step
     double *vd[VAH_NUM_VALIDITY];    // validity fields (FP64, ghosted layout)
     void *vq[16];                    // P_L, pi, Pi at the start of the step (validity input)
@@ -137,6 +138,7 @@ void free_all(vah_event *ev) {
     cudaFree(ev->d_counters);
     cudaFree(ev->d_fb);
     cudaFree(ev->d_stage64);
+    cudaFree(ev->d_stage_all);
     for (int m = 0; m < VAH_NUM_VALIDITY; ++m) cudaFree(ev->vd[m]);
     for (int n = 0; n < 16; ++n) cudaFree(ev->vq[n]);
     for (cudaEvent_t e : ev->tev) cudaEventDestroy(e);
@@ -438,6 +440,7 @@ extern "C" int vah_event_create(const vah_lattice *lat, const vah_hydro *hydro, 
     ev->steps = 0;
     ev->last_t = hydro->t0;
     ev->d_stage64 = nullptr;
+    ev->d_stage_all = nullptr;
     ev->d_fb = nullptr;
     ev->s_in = nullptr;
     ev->s_out = nullptr;
@@ -1277,21 +1280,181 @@ int step_host_pipelined(vah_event *ev, double t, double dt, double *const *field
     return vah_event_sync(ev);
 }
 
+// Every field of a host-buffer step at once (blockIdx.y: the field): FP64
+// host-layout rows [r0, r0 + rows) of hx values <-> FP32 device rows of the
+// padded pitch.
+struct FieldRows {
+    const void *src[VAH_NUM_FIELDS];
+    void *dst[VAH_NUM_FIELDS];
+};
+
+__global__ void narrow_rows_kernel(FieldRows f, int hx, int pitch, size_t r0, size_t rows) {
+    const double *src = (const double *)f.src[blockIdx.y] + r0 * hx;
+    float *dst = (float *)f.dst[blockIdx.y] + r0 * pitch;
+    const size_t n = (size_t)hx * rows;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        dst[(k / hx) * pitch + k % hx] = (float)src[k];
+}
+
+__global__ void widen_rows_kernel(FieldRows f, int hx, int pitch, size_t r0, size_t rows) {
+    const float *src = (const float *)f.src[blockIdx.y] + r0 * pitch;
+    double *dst = (double *)f.dst[blockIdx.y] + r0 * hx;
+    const size_t n = (size_t)hx * rows;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        dst[k] = (double)src[(k / hx) * pitch + k % hx];
+}
+
+// Slabs of whole tile layers along eta for the FP32 form's overlapped
+// host-buffer step: about `thick` planes each (rounded to tile layers, at
+// least one), as in slab_bounds. Returns the bounds in tile layers.
+std::vector<int> tile_slab_layers(int nz, int thick) {
+    constexpr int TZ = vah::TileShape<true>::TZ;
+    const int nlayer = (nz + TZ - 1) / TZ, per = std::max(1, (thick + TZ / 2) / TZ);
+    const int n = std::max(1, nlayer / per);
+    std::vector<int> b = {0};
+    for (int m = 0; m < n; ++m) b.push_back(b.back() + nlayer / n + (m < nlayer % n ? 1 : 0));
+    return b;
+}
+
+// Host-buffer step of the FP32 form (3+1D) with its copies overlapped, in the
+// slab order of step_host_pipelined. A slab is a run of whole tile layers, so
+// its tiles are one run of the k-major work-list, and its stage 1 or 2 is one
+// tile launch over that run. Its FP64 planes cross PCIe into a device copy of
+// the host layout (d_stage_all) and are narrowed into the FP32 fields on the
+// event's stream before its stage 1; after its stage 2 they are widened there
+// and copied back. Every slab but possibly the last has at least 4 planes, so
+// the 2-plane stencil halo of a slab lies in its neighbours, which is what the
+// order relies on.
+int step_host_fp32_pipelined(vah_event *ev, double t, double dt, double *const *fields, int thick) {
+    constexpr int TZ = vah::TileShape<true>::TZ, TX = vah::TileShape<true>::TX, TY = vah::TileShape<true>::TY;
+    const int nx = ev->lat.nx, ny = ev->lat.ny, nz = ev->lat.nz, hx = nx + 4;
+    const std::vector<int> lb = tile_slab_layers(nz, thick);
+    const int nslab = (int)lb.size() - 1, per_layer = ((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
+    auto plane_of = [&](int layer) { return std::min(layer * TZ, nz); };  // interior plane of a slab bound
+    const size_t hplane = (size_t)hx * ev->ncy, hn = hplane * ev->ncz;  // doubles per host plane, field
+    if (!ev->d_stage_all) VAH_TRY(cudaMalloc((void **)&ev->d_stage_all, VAH_NUM_FIELDS * hn * sizeof(double)));
+    if (!ev->s_in) VAH_TRY(cudaStreamCreateWithFlags(&ev->s_in, cudaStreamNonBlocking));
+    if (!ev->s_out) VAH_TRY(cudaStreamCreateWithFlags(&ev->s_out, cudaStreamNonBlocking));
+    while (ev->pev.size() < (size_t)(2 * nslab + 2)) {
+        cudaEvent_t e;
+        VAH_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ev->pev.push_back(e);
+    }
+    cudaEvent_t start = ev->pev[0], end = ev->pev[1], *in_ready = &ev->pev[2], *done = &ev->pev[2 + nslab];
+    // per field: the host array, its staging copy, the device field the step
+    // reads (narrowed into) and the one that holds it after the step (widened)
+    FieldRows in{}, out{};
+    double *host[VAH_NUM_FIELDS], *stg[VAH_NUM_FIELDS];
+    int nf = 0;
+    for (int id = 0; id < VAH_NUM_FIELDS; ++id) {
+        void *d = field_ptr(ev, id);
+        if (!d || !fields[id]) continue;
+        void *after = d;  // stage 2 writes u^{n+1} into the up buffer; u^n becomes up
+        if (id >= VAH_F_UT && id < VAH_F_UT + 4) after = ev->up[id - VAH_F_UT];
+        if (id >= VAH_F_UPT && id < VAH_F_UPT + 4) after = ev->u[id - VAH_F_UPT];
+        host[nf] = fields[id];
+        stg[nf] = ev->d_stage_all + (size_t)id * hn;
+        in.src[nf] = stg[nf];
+        in.dst[nf] = d;
+        out.src[nf] = after;
+        out.dst[nf] = stg[nf];
+        ++nf;
+    }
+    auto copy_planes = [&](bool to_device, size_t p0, size_t p1, cudaStream_t s) -> int {
+        if (p1 <= p0) return VAH_OK;
+        const size_t off = p0 * hplane, bytes = (p1 - p0) * hplane * sizeof(double);
+        for (int f = 0; f < nf; ++f) {
+            if (to_device)
+                VAH_TRY(cudaMemcpyAsync(stg[f] + off, host[f] + off, bytes, cudaMemcpyHostToDevice, s));
+            else
+                VAH_TRY(cudaMemcpyAsync(host[f] + off, stg[f] + off, bytes, cudaMemcpyDeviceToHost, s));
+        }
+        return VAH_OK;
+    };
+    auto convert = [&](bool narrow, size_t p0, size_t p1) -> int {
+        if (p1 <= p0 || nf == 0) return VAH_OK;
+        const size_t r0 = p0 * ev->ncy, rows = (p1 - p0) * ev->ncy;
+        const dim3 grid((unsigned)std::min<size_t>((rows * hx + 255) / 256, 148 * 4), (unsigned)nf);
+        if (narrow)
+            narrow_rows_kernel<<<grid, 256, 0, ev->stream>>>(in, hx, ev->ncx, r0, rows);
+        else
+            widen_rows_kernel<<<grid, 256, 0, ev->stream>>>(out, hx, ev->ncx, r0, rows);
+        VAH_TRY(cudaGetLastError());
+        return VAH_OK;
+    };
+    const vah::TileClock clk0{t, ev->tparity, 1, ev->steps};
+    const vah::Eos eos = make_eos(ev);
+    auto stage = [&](int st, int m) {
+        return vah::tile_launch(ev->d_tslot, nullptr, clk0, dt, ev->d_titems + (size_t)lb[m] * per_layer,
+                                (lb[m + 1] - lb[m]) * per_layer, true, ev->d_tcount, st, ev->opt.physics, eos,
+                                ev->d_terr, ev->stream);
+    };
+    VAH_TRY(cudaEventRecord(start, ev->stream));  // after the work queued before this step
+    VAH_TRY(cudaStreamWaitEvent(ev->s_in, start, 0));
+    VAH_TRY(cudaStreamWaitEvent(ev->s_out, start, 0));
+    size_t loaded = 0;  // ghosted planes [0, loaded) queued for copy-in and narrowed
+    int rc = VAH_OK;
+    for (int m = 0; m <= nslab && rc == VAH_OK; ++m) {
+        if (m < nslab) {
+            const size_t need = m == nslab - 1 ? (size_t)nz + 4 : (size_t)plane_of(lb[m + 1]) + 4;
+            rc = copy_planes(true, loaded, need, ev->s_in);
+            if (rc != VAH_OK) break;
+            VAH_TRY(cudaEventRecord(in_ready[m], ev->s_in));
+            VAH_TRY(cudaStreamWaitEvent(ev->stream, in_ready[m], 0));
+            rc = convert(true, loaded, need);
+            if (rc != VAH_OK) break;
+            loaded = need;
+            VAH_TRY(stage(1, m));
+        }
+        if (m >= 1) {
+            const int k = m - 1, lo = plane_of(lb[k]), hi = plane_of(lb[k + 1]);
+            VAH_TRY(stage(2, k));
+            const size_t p0 = k == 0 ? 0 : (size_t)lo + 2, p1 = k == nslab - 1 ? (size_t)nz + 4 : (size_t)hi + 2;
+            rc = convert(false, p0, p1);
+            if (rc != VAH_OK) break;
+            VAH_TRY(cudaEventRecord(done[k], ev->stream));
+            VAH_TRY(cudaStreamWaitEvent(ev->s_out, done[k], 0));
+            rc = copy_planes(false, p0, p1, ev->s_out);
+        }
+    }
+    // join the copy streams back into the event's stream, also on an error
+    if (cudaEventRecord(end, ev->s_out) == cudaSuccess) cudaStreamWaitEvent(ev->stream, end, 0);
+    if (cudaEventRecord(end, ev->s_in) == cudaSuccess) cudaStreamWaitEvent(ev->stream, end, 0);
+    if (rc != VAH_OK) return rc;
+    for (int m = 0; m < 4; ++m) {  // as vah_rk2_step
+        void *tmp = ev->u[m];
+        ev->u[m] = ev->up[m];
+        ev->up[m] = tmp;
+    }
+    ev->tparity ^= 1;
+    ev->steps++;
+    ev->last_t = t + dt;
+    ev->last_dt = dt;
+    return vah_event_sync(ev);
+}
+
 }  // namespace
 
 extern "C" int vah_rk2_step_host(vah_event *ev, double t, double dt, double *const *fields) {
     if (!ev || !fields) return VAH_ERR_ARG;
     VAH_TRY(cudaSetDevice(ev->opt.device));
     int rc;
-    if (ev->elem != sizeof(double)) return step_host_fp32(ev, t, dt, fields);
     // overlapped copies where the lattice has enough planes along eta (at
     // least 3 slabs); slab thickness from VAH_HOST_SLAB_PLANES (>= 2) when
-    // set, else nz / 6 (6 slabs: the best of 3 to 40 on the 121x121x81 event)
+    // set, else nz / 6 (6 slabs: the best of 3 to 40 on the 121x121x81 event;
+    // the FP32 form rounds it to whole tile layers)
     static const int slab_env = [] {
         const char *v = getenv("VAH_HOST_SLAB_PLANES");
         return v ? atoi(v) : 0;
     }();
     const int slab = slab_env >= 2 ? slab_env : std::max(2, ev->lat.nz / 6);
+    if (ev->elem != sizeof(double)) {
+        if (ev->lat.nz > 1 && !ev->validity && tile_slab_layers(ev->lat.nz, slab).size() >= 4) {
+            if (!(dt > 0) || !(t > 0)) return VAH_ERR_ARG;
+            return step_host_fp32_pipelined(ev, t, dt, fields, slab);
+        }
+        return step_host_fp32(ev, t, dt, fields);
+    }
     if (ev->opt.flux != VAH_FLUX_PER_CELL_FUSED && !ev->validity && ev->lat.nz >= 3 * slab) {
         if (!(dt > 0) || !(t > 0)) return VAH_ERR_ARG;
         return step_host_pipelined(ev, t, dt, fields, slab);

@@ -270,16 +270,20 @@ int vah_event_autotune(vah_event *ev, int reps, vah_tune_report *out);
  * (FullyDiscreteKurganovTadmorScheme.h:13-15). `fields` holds
  * VAH_NUM_FIELDS pointers; unused physics slots may be NULL. With FP32
  * storage the arrays still cross as FP64 and are narrowed (widened on the
- * way back) by a kernel, through one field of device staging that the first
- * such call allocates.
+ * way back) by a kernel, through device staging in the host layout that the
+ * first such call allocates (one field; every field where the copies
+ * overlap).
  * FP64 storage, face/cell split, validity off and nz >= 6: the copies
  * overlap the stages. The lattice is cut into slabs of planes along eta
  * (VAH_HOST_SLAB_PLANES planes each when that environment variable is set to
  * 2 or more, else nz / 6); copy-in of later slabs, the stages of earlier ones
  * and copy-out of finished ones run on three streams (the event's stream and
- * two the first such call creates), with the same results bit for bit. The
- * arrays should be pinned (cudaHostAlloc / cudaHostRegister) for the
- * copies to overlap; pageable arrays give the same results, more slowly. */
+ * two the first such call creates), with the same results bit for bit.
+ * FP32 storage, 3+1D, validity off: the same, in slabs of whole 4-plane tile
+ * layers (the thickness above rounded to layers), where that gives at least
+ * 3 slabs. The arrays should be pinned (cudaHostAlloc / cudaHostRegister)
+ * for the copies to overlap; pageable arrays give the same results, more
+ * slowly. */
 int vah_rk2_step_host(vah_event *ev, double t, double dt, double *const *fields);
 
 /* ---- batches: many events of uneven size in one launch per kernel kind ----

@@ -257,6 +257,40 @@ def test_gpu_host_buffer_step_fp32_storage_matches_device_step():
     ev.close()
 
 
+@pytest.mark.parametrize("nz", [9, 23, 41])
+def test_gpu_host_buffer_step_fp32_overlapped_slabs_match_device_step(nz):
+    """FP32 form, 3+1D: host-buffer steps take the overlapped path, in slabs
+    of whole 4-plane tile layers (nz = 9: 4, 4, 1 planes; nz = 23: 4 x 5, 3;
+    nz = 41: 12, 8, 8, 8, 5), each slab's stage one tile launch over its run
+    of the work-list, its planes narrowed after their copy-in and widened
+    before their copy-out. Two steps in a row equal set_field + step +
+    get_field bit for bit on every field, ghosts included."""
+    tab = V.eos_table()
+    nx, ny = 25, 23
+    g = V.Grid(nx, ny, nz, 0.1 * 121 / nx, 0.1 * 121 / ny, 0.1, 0.16, physics="pimunu_pi", eos="table",
+               zeta="crossover", table=tab)
+    e_peak = V.product.table_energy_density(tab, 0.6 / 0.197326938)
+    exy, _ = V.product.mc_glauber(nx, ny, g.dx, g.dy, 7.0, seed=5, e_peak=e_peak)
+    e3 = (V.product.longitudinal(nz, g.dz)[:, None] * exy[None, :]).ravel()
+    ev = V.Event(g, t0=0.25, precision=1)
+    ev.init_from_e(0.25, e3, 1)
+    ev.run(0.25, 0.005, 4)
+    ids = list(range(V.NUM_FIELDS))
+    state0 = {fid: ev.get_field(fid) for fid in ids}
+    state = {fid: a.copy() for fid, a in state0.items()}
+    ptrs = [state[fid].ctypes.data for fid in range(V.NUM_FIELDS)]
+    ev.step_host(0.27, 0.005, ptrs)
+    ev.step_host(0.275, 0.005, ptrs)
+    dev = V.Event(g, t0=0.25, precision=1)
+    upload(dev, g, state0)
+    dev.step(0.27, 0.005)
+    dev.step(0.275, 0.005)
+    for fid in ids:
+        np.testing.assert_array_equal(state[fid], dev.get_field(fid), err_msg=f"field {fid}")
+    dev.close()
+    ev.close()
+
+
 def test_gpu_nan_is_reported_not_fatal():
     g, e2 = conformal_workload(9, 9)
     ev = V.Event(g, t0=0.5)
