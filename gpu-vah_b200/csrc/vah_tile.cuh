@@ -15,13 +15,13 @@
 // a 4-D TMA load (cp.async.bulk.tensor: x, y, z and all N_q fields) of the
 // tile plus a 2-cell halo of the stage-input conserved fields into shared
 // memory, and two more of e, p and u^mu with a 1-cell halo, completed on an
-// mbarrier. The faces of the tile are then evaluated once each into registers
-// and shared memory (x: in registers, exchanged with the neighbour cell
-// through warp shuffles; y and z: a shared face buffer; the tile's lower
-// boundary faces: a second small buffer, evaluated by threads 0-127 in the
-// first of the two face phases so that every thread evaluates at most four
-// faces), every cell takes its flux differences from there and runs its
-// explicit update. Then the next tile's copies are issued, and they land
+// mbarrier. The faces of the tile are then evaluated once each, from one
+// inlined call site in a loop over four jobs: the tile's lower boundary faces
+// (threads 0-127, into a small shared buffer), then every cell's +1/2 face
+// along x (differenced at once with the neighbour cell's through warp
+// shuffles), along y and along z (a shared face buffer, differenced after a
+// barrier), so that only the flux differences stay live between jobs. Every
+// cell then runs its explicit update. Then the next tile's copies are issued, and they land
 // while this tile's cells run their FP64 inversions, regulator and stores.
 // Face fluxes never leave the SM.
 //
@@ -52,7 +52,7 @@ struct TileShape {
     static constexpr int NBX = TY * TZ, NBY = TX * TZ, NBZ = IS3D ? TX * TY : 0;  // lower boundary faces per axis
     static constexpr int NBXY = NBX + NBY;
     static_assert(TX * TY * TZ == kTileThreads, "one thread per cell");
-    static_assert(NBXY + NBZ <= kTileThreads, "boundary faces: one per thread, all in the first face phase");
+    static_assert(NBXY + NBZ <= kTileThreads, "boundary faces: one per thread, all in the first face job");
     static_assert((BX * 4) % 16 == 0, "TMA box rows must be a multiple of 16 bytes");
 };
 
@@ -161,6 +161,23 @@ __device__ __forceinline__ void tile_count(unsigned long long *c, unsigned v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(c, (unsigned long long)s);
+}
+
+// flux[n] = c (hm[n] - hp[n]) (ACC: flux[n] += ...) over the N_q fields, two
+// at a time.
+template <int NQ, bool ACC>
+__device__ __forceinline__ void flux_diff(float *flux, float c, const float *hm, const float *hp) {
+#pragma unroll
+    for (int n = 0; n + 1 < NQ; n += 2) {
+        const Pair d = psub(Pair{hm[n], hm[n + 1]}, Pair{hp[n], hp[n + 1]});
+        const Pair f = ACC ? pfma(Pair{c, c}, d, Pair{flux[n], flux[n + 1]}) : pmul(Pair{c, c}, d);
+        flux[n] = f.a;
+        flux[n + 1] = f.b;
+    }
+    if (NQ % 2) {
+        const float d = hm[NQ - 1] - hp[NQ - 1];
+        flux[NQ - 1] = ACC ? fmaf(c, d, flux[NQ - 1]) : c * d;
+    }
 }
 
 // The dynamic shared memory of one block: the TMA boxes (conserved fields,
@@ -272,67 +289,89 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         const double e0 = (double)sE[pc], ux0 = (double)sUX[pc], uy0 = (double)sUY[pc];
         const double uT0 = sqrt(fabs(ux0 * ux0 + uy0 * uy0));
 
-        // lower boundary face b of the tile along `dir` into dst (stride ds);
-        // the left cell is in the halo
-        auto boundary = [&](int b, int dir, float *dst, int ds) {
-            int bi, bj, bk;  // left cell in the conserved box
-            if (dir == 0) { bi = 1; bj = 2 + b % TY; bk = IS3D ? 2 + b / TY : 0; }
-            else if (dir == 1) { bi = 2 + b % TX; bj = 1; bk = IS3D ? 2 + b / TX : 0; }
-            else { bi = 2 + b % TX; bj = 2 + b / TX; bk = 1; }
-            const int ri = it.i0 + bi - 2 + (dir == 0), rj = it.j0 + bj - 2 + (dir == 1),
-                      rk = it.k0 + (IS3D ? bk - 2 : 0) + (dir == 2);  // the right cell: the tile's first
-            if (ri < d.nx && rj < d.ny && rk < d.nz) {
-                const int pl = bi + PBX * ((bj - 1) + PBY * (IS3D ? bk - 1 : 0));
-                const double el = (double)sE[pl], ux = (double)sUX[pl], uy = (double)sUY[pl];
-                count(tile_face<PHYS>(bq, bi + BX * (bj + BY * bk), dir == 0 ? 1 : (dir == 1 ? SY : SZ), dir, t_src, el,
-                                      sqrt(fabs(ux * ux + uy * uy)), dst, ds));
-            } else {
-#pragma unroll
-                for (int n = 0; n < NQ; ++n) dst[n * ds] = 0.0f;
-            }
-        };
-
-        // ---- faces, phase 1: +1/2 along x (registers) and y (face buffer); the
-        // lower boundary faces along x and y (threads 0 .. NBXY-1) and, in
-        // 3+1D, along z (the next NBZ threads), so that no thread evaluates
-        // more than three faces in this phase and one in the next ----
-        float Hx[NQ];
-        if (live) count(tile_face<PHYS>(bq, bc, 1, 0, t_src, e0, uT0, Hx, 1));
-        else
-#pragma unroll
-            for (int n = 0; n < NQ; ++n) Hx[n] = 0.0f;
-        if (tid < SH::NBXY) boundary(tid < SH::NBX ? tid : tid - SH::NBX, tid < SH::NBX ? 0 : 1, sB + tid, SH::NBXY);
-        else if (IS3D && tid < SH::NBXY + SH::NBZ)
-            boundary(tid - SH::NBXY, 2, sB + SH::NBXY * NQ + (tid - SH::NBXY), SH::NBZ);
-        if (live) count(tile_face<PHYS>(bq, bc, SY, 1, t_src, e0, uT0, sF + tid, kTileThreads));
-        else
-#pragma unroll
-            for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = 0.0f;
-        __syncthreads();
-
-        // flux differences: x through warp shuffles (lane - 1 holds the -1/2
-        // face), y from the face buffer
+        // ---- faces: one evaluation site, in four jobs --
+        //   0: the lower boundary face of the tile that this thread owns
+        //      (threads 0 .. NBXY + NBZ - 1: x, y, then z faces) into sB;
+        //   1: +1/2 along x, differenced at once through warp shuffles (the
+        //      -1/2 face from lane - 1, or from sB at the tile's edge);
+        //   2: +1/2 along y into the face buffer, differenced after a barrier;
+        //   3: (3+1D) +1/2 along z, the same, reusing the face buffer.
+        // Nothing but the flux differences stays live from one job to the next.
         const float cx = (float)(dt / d.dx), cy = (float)(dt / d.dy), cz = (float)(dt / d.dz);
         float flux[NQ];
-#pragma unroll
-        for (int n = 0; n < NQ; ++n) {
-            float hm = __shfl_up_sync(0xffffffffu, Hx[n], 1, TX);
-            if (lx == 0) hm = sB[n * SH::NBXY + (ly + TY * lz)];
-            const float ym = ly > 0 ? sF[n * kTileThreads + tid - TX] : sB[n * SH::NBXY + SH::NBX + lx + TX * lz];
-            flux[n] = cx * (hm - Hx[n]) + cy * (ym - sF[n * kTileThreads + tid]);
-        }
-        if (IS3D) {  // phase 2: +1/2 along z (reusing the face buffer)
-            __syncthreads();
-            if (live) count(tile_face<PHYS>(bq, bc, SZ, 2, t_src, e0, uT0, sF + tid, kTileThreads));
+        constexpr int NB = SH::NBXY + SH::NBZ;
+        constexpr int NJOB = IS3D ? 4 : 3;
+#pragma unroll 1
+        for (int job = 0; job < NJOB; ++job) {
+            if (job == 1 || job == 3) __syncthreads();  // 1: boundary faces written; 3: y differences read
+            bool act = live, store = true;
+            int l = bc, st = 1, dir = job == 2 ? 1 : (job == 3 ? 2 : 0);
+            if (job == 2) st = SY;
+            if (job == 3) st = SZ;
+            double eP = e0, ug = uT0;
+            float *dst = sF + tid;
+            int ds = kTileThreads;
+            if (job == 0) {
+                store = tid < NB;
+                act = false;
+                if (store) {
+                    const int bdir = tid < SH::NBX ? 0 : (tid < SH::NBXY ? 1 : 2);
+                    const int b = bdir == 0 ? tid : (bdir == 1 ? tid - SH::NBX : tid - SH::NBXY);
+                    int bi, bj, bk;  // left cell in the conserved box (in the halo)
+                    if (bdir == 0) { bi = 1; bj = 2 + b % TY; bk = IS3D ? 2 + b / TY : 0; }
+                    else if (bdir == 1) { bi = 2 + b % TX; bj = 1; bk = IS3D ? 2 + b / TX : 0; }
+                    else { bi = 2 + b % TX; bj = 2 + b / TX; bk = 1; }
+                    const int ri = it.i0 + bi - 2 + (bdir == 0), rj = it.j0 + bj - 2 + (bdir == 1),
+                              rk = it.k0 + (IS3D ? bk - 2 : 0) + (bdir == 2);  // the right cell: the tile's first
+                    act = ri < d.nx && rj < d.ny && rk < d.nz;
+                    l = bi + BX * (bj + BY * bk);
+                    st = bdir == 0 ? 1 : (bdir == 1 ? SY : SZ);
+                    dir = bdir;
+                    const int pl = bi + PBX * ((bj - 1) + PBY * (IS3D ? bk - 1 : 0));
+                    eP = (double)sE[pl];
+                    const double ux = (double)sUX[pl], uy = (double)sUY[pl];
+                    ug = sqrt(fabs(ux * ux + uy * uy));
+                    dst = bdir < 2 ? sB + tid : sB + SH::NBXY * NQ + (tid - SH::NBXY);
+                    ds = bdir < 2 ? SH::NBXY : SH::NBZ;
+                }
+            }
+            float Hj[NQ];
+            if (act) count(tile_face<PHYS>(bq, l, st, dir, t_src, eP, ug, Hj, 1));
             else
 #pragma unroll
-                for (int n = 0; n < NQ; ++n) sF[n * kTileThreads + tid] = 0.0f;
-            __syncthreads();
-            const float *sBz = sB + SH::NBXY * NQ;
+                for (int n = 0; n < NQ; ++n) Hj[n] = 0.0f;
+            if (job == 1) {  // x: lane - 1 holds the -1/2 face
+                float hm[NQ];
 #pragma unroll
-            for (int n = 0; n < NQ; ++n) {
-                const float zm = lz > 0 ? sF[n * kTileThreads + tid - TX * TY] : sBz[n * SH::NBZ + lx + TX * ly];
-                flux[n] += cz * (zm - sF[n * kTileThreads + tid]);
+                for (int n = 0; n < NQ; ++n) {
+                    hm[n] = __shfl_up_sync(0xffffffffu, Hj[n], 1, TX);
+                    if (lx == 0) hm[n] = sB[n * SH::NBXY + (ly + TY * lz)];
+                }
+                flux_diff<NQ, false>(flux, cx, hm, Hj);
+            } else {
+                if (store)
+#pragma unroll
+                    for (int n = 0; n < NQ; ++n) dst[n * ds] = Hj[n];
+                if (job >= 2) {
+                    __syncthreads();
+                    float hm[NQ], hp[NQ];
+                    if (job == 2) {
+#pragma unroll
+                        for (int n = 0; n < NQ; ++n) {
+                            hm[n] = ly > 0 ? sF[n * kTileThreads + tid - TX] : sB[n * SH::NBXY + SH::NBX + lx + TX * lz];
+                            hp[n] = sF[n * kTileThreads + tid];
+                        }
+                        flux_diff<NQ, true>(flux, cy, hm, hp);
+                    } else {
+                        const float *sBz = sB + SH::NBXY * NQ;
+#pragma unroll
+                        for (int n = 0; n < NQ; ++n) {
+                            hm[n] = lz > 0 ? sF[n * kTileThreads + tid - TX * TY] : sBz[n * SH::NBZ + lx + TX * ly];
+                            hp[n] = sF[n * kTileThreads + tid];
+                        }
+                        flux_diff<NQ, true>(flux, cz, hm, hp);
+                    }
+                }
             }
         }
         if (d.counters) {

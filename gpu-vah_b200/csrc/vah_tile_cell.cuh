@@ -6,17 +6,54 @@
 
 #include "vah_physics.cuh"
 
-// The face evaluation is called from four places per tile; kept out of line
-// on the device so that the kernel's code fits the instruction cache.
-#if defined(__CUDACC__) && !defined(VAH_TILE_FACE_INLINE)
-#define VAH_TILE_FACE __host__ __device__ __noinline__
-#elif defined(__CUDACC__)
+// The face evaluation is inlined: the tile kernel calls it from one place (a
+// loop over the face jobs of a tile), so one copy of its code sits in the
+// kernel and no call saves registers around it.
+#if defined(__CUDACC__)
 #define VAH_TILE_FACE __host__ __device__ __forceinline__
 #else
 #define VAH_TILE_FACE inline
 #endif
 
 namespace vah {
+
+// Two FP32 lanes per instruction: sm_100's paired FFMA2 / FMUL2, each lane
+// rounded as its scalar operation; on the host one operation per lane.
+struct Pair {
+    float a, b;
+};
+VAH_HD Pair pfma(Pair x, Pair y, Pair z) {
+#ifdef __CUDA_ARCH__
+    const float2 r = __ffma2_rn(make_float2(x.a, x.b), make_float2(y.a, y.b), make_float2(z.a, z.b));
+    return {r.x, r.y};
+#else
+    return {fmaf(x.a, y.a, z.a), fmaf(x.b, y.b, z.b)};
+#endif
+}
+VAH_HD Pair pmul(Pair x, Pair y) {
+#ifdef __CUDA_ARCH__
+    const float2 r = __fmul2_rn(make_float2(x.a, x.b), make_float2(y.a, y.b));
+    return {r.x, r.y};
+#else
+    return {x.a * y.a, x.b * y.b};
+#endif
+}
+// x - y, rounded once (y times -1 is exact)
+VAH_HD Pair psub(Pair x, Pair y) { return pfma(y, Pair{-1.0f, -1.0f}, x); }
+
+// approx_derivative of two fields at once: the differences and products
+// paired, the minima and sign tests per lane; the same values bit for bit.
+VAH_HD Pair approx_derivative2(Pair x, Pair y, Pair z) {
+    const Pair dl = psub(y, x), dr = psub(z, y);
+    const Pair c = pmul(psub(z, x), Pair{0.5f, 0.5f});
+    const Pair mn = pmul(Pair{1.1f, 1.1f}, Pair{fminf(fabsf(dl.a), fabsf(dr.a)), fminf(fabsf(dl.b), fabsf(dr.b))});
+    auto pick = [](float l, float r, float cc, float mm) {
+        const float m = fminf(mm, fabsf(cc));
+        const bool neg = l < 0.0f;
+        return neg == (r < 0.0f) ? (neg ? -m : m) : 0.0f;
+    };
+    return {pick(dl.a, dr.a, c.a, mn.a), pick(dl.b, dr.b, c.b, mn.b)};
+}
 
 // --------------------------------------------- the FP32 form's cell algebra --
 // Host-and-device code: the kernel runs it on the shared-memory box, and the
@@ -49,10 +86,21 @@ VAH_TILE_FACE unsigned tile_face(const QA q, long long L, long long st, int dir,
     constexpr int NQ = Phys<PHYS>::NQ;
     float qR[NQ], qL[NQ];
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) {
+    for (int n = 0; n + 1 < NQ; n += 2) {  // two fields at a time
+        const Pair qm{q(n, L - st), q(n + 1, L - st)}, q0{q(n, L), q(n + 1, L)};
+        const Pair qp{q(n, L + st), q(n + 1, L + st)}, qpp{q(n, L + 2 * st), q(n + 1, L + 2 * st)};
+        const Pair r = pfma(approx_derivative2(q0, qp, qpp), Pair{-0.5f, -0.5f}, qp);
+        const Pair l = pfma(approx_derivative2(qm, q0, qp), Pair{0.5f, 0.5f}, q0);
+        qR[n] = r.a;
+        qR[n + 1] = r.b;
+        qL[n] = l.a;
+        qL[n + 1] = l.b;
+    }
+    if (NQ % 2) {
+        constexpr int n = NQ - 1;
         const float qm = q(n, L - st), q0 = q(n, L), qp = q(n, L + st), qpp = q(n, L + 2 * st);
-        qR[n] = qp - approx_derivative(q0, qp, qpp) * 0.5f;
-        qL[n] = q0 + approx_derivative(qm, q0, qp) * 0.5f;
+        qR[n] = fmaf(approx_derivative(q0, qp, qpp), -0.5f, qp);
+        qL[n] = fmaf(approx_derivative(qm, q0, qp), 0.5f, q0);
     }
     double dR[16], dL[16];
 #pragma unroll
@@ -71,7 +119,12 @@ VAH_TILE_FACE unsigned tile_face(const QA q, long long L, long long st, int dir,
     const double a = fmax(fabs(vL), fabs(vR));
     const float wR = (float)(0.5 * (vR - a)), wL = (float)(0.5 * (vL + a));
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) H[n * hs] = wR * qR[n] + wL * qL[n];
+    for (int n = 0; n + 1 < NQ; n += 2) {  // wR qR + wL qL, two fields at a time
+        const Pair h = pfma(Pair{wR, wR}, Pair{qR[n], qR[n + 1]}, pmul(Pair{wL, wL}, Pair{qL[n], qL[n + 1]}));
+        H[n * hs] = h.a;
+        H[(n + 1) * hs] = h.b;
+    }
+    if (NQ % 2) H[(NQ - 1) * hs] = fmaf(wR, qR[NQ - 1], wL * qL[NQ - 1]);
     return (stR != 0) + (stL != 0) + ((stR == 2 || stL == 2) ? 256u : 0u);
 }
 
