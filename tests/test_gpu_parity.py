@@ -257,13 +257,14 @@ def test_gpu_host_buffer_step_fp32_storage_matches_device_step():
     ev.close()
 
 
-@pytest.mark.parametrize("nz", [9, 23, 41])
+@pytest.mark.parametrize("nz", [5, 9, 23, 41])
 def test_gpu_host_buffer_step_fp32_overlapped_slabs_match_device_step(nz):
     """FP32 form, 3+1D: host-buffer steps take the overlapped path, in slabs
     of whole 4-plane tile layers (nz = 9: 4, 4, 1 planes; nz = 23: 4 x 5, 3;
     nz = 41: 12, 8, 8, 8, 5), each slab's stage one tile launch over its run
     of the work-list, its planes narrowed after their copy-in and widened
-    before their copy-out. Two steps in a row equal set_field + step +
+    before their copy-out; nz = 5 (two tile layers, fewer than three slabs)
+    takes the plain path. Two steps in a row equal set_field + step +
     get_field bit for bit on every field, ghosts included."""
     tab = V.eos_table()
     nx, ny = 25, 23
