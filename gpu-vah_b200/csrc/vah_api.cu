@@ -185,6 +185,10 @@ void fill_common(const vah_event *ev, StageArgs<S> &a) {
             a.H[d][n] = (S *)ev->H[d][n];
             a.HR[d][n] = (S *)ev->HR[d][n];
         }
+    // FP64 face/cell split: the x face launch writes each cell's x flux
+    // difference into the x face scratch, and the cell launch reads that
+    if (sizeof(S) == sizeof(double) && ev->opt.flux != VAH_FLUX_PER_CELL_FUSED)
+        for (int n = 0; n < 16; ++n) a.Dx[n] = (S *)ev->H[0][n];
     if (ev->validity)
         for (int m = 0; m < 11; ++m) a.regmap[m] = ev->vd[VAH_V_REGULATIONS + m];
 }

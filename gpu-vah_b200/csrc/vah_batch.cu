@@ -114,6 +114,7 @@ __device__ void make_args(StageArgs<S> &a, const SlotDesc<S> &d, const SlotClock
             a.H[k][n] = d.H[k][n];
             a.HR[k][n] = d.HR[k][n];
         }
+    for (int n = 0; n < 16; ++n) a.Dx[n] = nullptr;  // the batch's cell launch differences H / HR itself
     finish_args(a);
 }
 

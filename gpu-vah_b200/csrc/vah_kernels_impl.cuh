@@ -65,6 +65,59 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) face_kernel(const StageAr
     }
 }
 
+// Faces along x with the x flux differences taken in the launch (a.Dx set):
+// blocks of 32 x 4 threads, one warp per row segment. Lane L of warp w in its
+// row takes the face at +1/2 of ghosted cell f + 1, f = 31 w + L, so that
+// consecutive warps share one face. Each face is evaluated as in face_kernel,
+// but only the two evaluations' weights are kept, and each field's two fluxes
+// are formed at the exchange: lane L >= 1 owns cell f + 1 (when interior) and
+// writes Dx = H(-1/2) - H(+1/2) as that cell evaluates them, the -1/2 value
+// from lane L - 1 through a shuffle. The face a warp shares with the previous
+// one is evaluated twice and counted once.
+template <typename S, int PHYS, bool EXACT, int MINB>
+__global__ void __launch_bounds__(kSplitThreads, MINB) face_x_diff_kernel(const StageArgs<S> a) {
+    constexpr int NQ = Phys<PHYS>::NQ;
+    const int lane = threadIdx.x;  // blockDim.x == 32: a warp is one row segment
+    const int r = row_block() * blockDim.y + threadIdx.y;
+    if (r >= a.ny * (a.k1 - a.k0)) return;  // whole warps
+    const int j = r % a.ny, k = r / a.ny + a.k0;
+    const int gi = 31 * blockIdx.x + lane + 1;  // the face at +1/2 of ghosted cell gi
+    const bool act = gi <= a.nx + 1;            // faces 1 .. nx + 1 bound the interior cells
+    const long long s = gi + (long long)a.ncx * (j + 2) + a.plane * (k + 2);
+    double qR[NQ], qL[NQ];
+    double wRo = 0.0, wLo = 0.0, wRr = 0.0, wLr = 0.0;  // the left cell's evaluation, the right cell's
+    unsigned fails = 0;
+    if (act) {
+        face_states<S, PHYS>(a, s, 1, qR, qL);
+        InvSetup sR, sL;
+        invert_setup<PHYS>(a.t_src, qR, sR);
+        invert_setup<PHYS>(a.t_src, qL, sL);
+        if (!EXACT || gi >= 2) {
+            const double ux = ld(a.uin[1], s), uy = ld(a.uin[2], s);
+            fails += face_weights(sR, sL, 0, ld(a.ein, s), sqrt(fabs(ux * ux + uy * uy)), wRo, wLo);
+        }
+        if (EXACT && gi <= a.nx) {
+            const double vx = ld(a.uin[1], s + 1), vy = ld(a.uin[2], s + 1);
+            fails += face_weights(sR, sL, 0, ld(a.ein, s + 1), sqrt(fabs(vx * vx + vy * vy)), wRr, wLr);
+        }
+    } else {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) qR[n] = qL[n] = 0.0;
+    }
+    const bool own = act && lane >= 1 && gi >= 2;  // cell gi is interior, and lane - 1 holds its -1/2 face
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) {
+        const double h = wRo * qR[n] + wLo * qL[n];                 // +1/2 as cell gi evaluates it
+        const double hr = EXACT ? wRr * qR[n] + wLr * qL[n] : h;   // +1/2 as cell gi + 1 evaluates it
+        const double hm = __shfl_up_sync(0xffffffffu, hr, 1);
+        if (own) a.Dx[n][s] = (S)(hm - h);
+    }
+    if (a.counters && act && (lane >= 1 || blockIdx.x == 0)) {
+        if (fails & 255u) count_add(a.counters + 0, fails & 255u);
+        if (fails >> 8) count_add(a.counters + 2, 1ull);
+    }
+}
+
 template <typename S, int PHYS, bool IS3D, bool EXACT, int MINB>
 __global__ void __launch_bounds__(kSplitThreads, MINB) cell_kernel(const StageArgs<S> a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,6 +223,21 @@ cudaError_t face_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t
     return cudaGetLastError();
 }
 
+// The x face launch that also differences (a.Dx set): 32 x 4 blocks whatever
+// the tuned shape (a warp must be one row segment); the register cap as tuned.
+template <typename S, int PHYS, bool EXACT>
+cudaError_t face_x_diff_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t stream) {
+    const int rows = a.ny * (a.k1 - a.k0);
+    const dim3 block(32, kSplitThreads / 32), grid = row_grid((a.nx + 30) / 31, rows, 1, kSplitThreads / 32);
+    switch (c.minb) {
+    case 3: face_x_diff_kernel<S, PHYS, EXACT, 3><<<grid, block, 0, stream>>>(a); break;
+    case 4: face_x_diff_kernel<S, PHYS, EXACT, 4><<<grid, block, 0, stream>>>(a); break;
+    case 5: face_x_diff_kernel<S, PHYS, EXACT, 5><<<grid, block, 0, stream>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 template <typename S, int PHYS, bool EXACT, bool IS3D>
 cudaError_t cell_launch(const StageArgs<S> &a, const KindConfig &c, cudaStream_t stream) {
     const dim3 block(c.bx, c.by), grid = row_grid(a.nx, (long long)a.ny * (a.k1 - a.k0), c.bx, c.by);
@@ -187,7 +255,7 @@ cudaError_t split_kind_dispatch(const StageArgs<S> &a, int kind, const KindConfi
     if (a.k0 < 0 || a.k1 > a.nz || a.k0 > a.k1) return cudaErrorInvalidValue;
     if (a.k0 == a.k1) return cudaSuccess;  // no planes
     switch (kind) {
-    case kFaceX: return face_launch<S, PHYS, EXACT, 0>(a, c, stream);
+    case kFaceX: return a.Dx[0] ? face_x_diff_launch<S, PHYS, EXACT>(a, c, stream) : face_launch<S, PHYS, EXACT, 0>(a, c, stream);
     case kFaceY: return face_launch<S, PHYS, EXACT, 1>(a, c, stream);
     case kFaceZ: return a.nz > 1 ? face_launch<S, PHYS, EXACT, 2>(a, c, stream) : cudaSuccess;
     case kCell:

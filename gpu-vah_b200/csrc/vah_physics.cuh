@@ -476,10 +476,9 @@ VAH_HD int face_velocity_of(const InvSetup &s, double uT, int dir, double *v) {
     return (isnan(vv) || isnan(s.c0)) ? 2 : 0;
 }
 
-template <int PHYS>
-VAH_HD int face_flux_setup(const InvSetup &sR, const InvSetup &sL, const double *qR, const double *qL, int dir,
-                           double ePrev, double uT, double *H) {
-    constexpr int NQ = Phys<PHYS>::NQ;
+// The weights of one evaluation, H = wR qR + wL qL (the same statuses).
+VAH_HD int face_weights(const InvSetup &sR, const InvSetup &sL, int dir, double ePrev, double uT, double &wR,
+                        double &wL) {
     // both states' Newton solves from this guess, in lockstep
     double uR, uL, vR = 0.0, vL = 0.0;
     int nR, nL;
@@ -488,10 +487,20 @@ VAH_HD int face_flux_setup(const InvSetup &sR, const InvSetup &sL, const double 
     const int stL = nL != 0 ? (isnan(ePrev) ? 2 : 1) : face_velocity_of(sL, uL, dir, &vL);
     const double a = fmax(fabs(vL), fabs(vR));
     // (vR qR + vL qL - a (qR - qL)) / 2 = wR qR + wL qL; the halving is exact
-    const double wR = 0.5 * (vR - a), wL = 0.5 * (vL + a);
+    wR = 0.5 * (vR - a);
+    wL = 0.5 * (vL + a);
+    return (stR != 0) + (stL != 0) + ((stR == 2 || stL == 2) ? 256 : 0);
+}
+
+template <int PHYS>
+VAH_HD int face_flux_setup(const InvSetup &sR, const InvSetup &sL, const double *qR, const double *qL, int dir,
+                           double ePrev, double uT, double *H) {
+    constexpr int NQ = Phys<PHYS>::NQ;
+    double wR, wL;
+    const int st = face_weights(sR, sL, dir, ePrev, uT, wR, wL);
 #pragma unroll
     for (int n = 0; n < NQ; ++n) H[n] = wR * qR[n] + wL * qL[n];
-    return (stR != 0) + (stL != 0) + ((stR == 2 || stL == 2) ? 256 : 0);
+    return st;
 }
 
 template <int PHYS>

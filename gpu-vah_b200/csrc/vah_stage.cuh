@@ -56,6 +56,11 @@ struct StageArgs {
     // reference face semantics only); scratch of ncell entries per field
     S *H[3][16];
     S *HR[3][16];
+    // optional (FP64 event launches): the x flux difference of each interior
+    // cell, H(-1/2) - H(+1/2) as the cell evaluates both faces, written by the
+    // x face launch (face_x_diff_kernel) and read by the cell launch instead of
+    // H[0] / HR[0]; null: the cell launch differences H[0] / HR[0] itself
+    S *Dx[16];
 };
 
 VAH_HD void count_add(unsigned long long *c, unsigned long long v) {
@@ -262,11 +267,10 @@ VAH_HD void stage_cell(const StageArgs<S> &a, int i, int j, int k) {
 // reference faces only interior cells' evaluations are needed (and counted,
 // as the reference counts them): the evaluation with a ghost cell's guess at
 // the first and last face of a row is skipped.
-template <typename S, int PHYS, bool EXACT>
-VAH_HD unsigned face_compute(const StageArgs<S> &a, long long s, int dir, long long st, bool left_in = true,
-                             bool right_in = true) {
+// The two reconstructed states at the face at +1/2 of ghosted cell s (stride st).
+template <typename S, int PHYS>
+VAH_HD void face_states(const StageArgs<S> &a, long long s, long long st, double *qR, double *qL) {
     constexpr int NQ = Phys<PHYS>::NQ;
-    double qR[NQ], qL[NQ], H[NQ];
 #pragma unroll
     for (int n = 0; n < NQ; ++n) {
         const double qm = ld(a.qin[n], s - st), q0 = ld(a.qin[n], s), qp = ld(a.qin[n], s + st),
@@ -274,6 +278,14 @@ VAH_HD unsigned face_compute(const StageArgs<S> &a, long long s, int dir, long l
         qR[n] = qp - approx_derivative(q0, qp, qpp) * 0.5;
         qL[n] = q0 + approx_derivative(qm, q0, qp) * 0.5;
     }
+}
+
+template <typename S, int PHYS, bool EXACT>
+VAH_HD unsigned face_compute(const StageArgs<S> &a, long long s, int dir, long long st, bool left_in = true,
+                             bool right_in = true) {
+    constexpr int NQ = Phys<PHYS>::NQ;
+    double qR[NQ], qL[NQ], H[NQ];
+    face_states<S, PHYS>(a, s, st, qR, qL);
     InvSetup sR, sL;  // set up once, inverted from one guess (shared) or both (reference faces)
     invert_setup<PHYS>(a.t_src, qR, sR);
     invert_setup<PHYS>(a.t_src, qL, sL);
@@ -314,8 +326,13 @@ VAH_HD void cell_compute(const StageArgs<S> &a, int i, int j, int k) {
         const long long st = strides[dir];
         const double c = a.c_h[dir];
         const S *const *Hm = EXACT ? a.HR[dir] : a.H[dir];  // face -1/2 as this cell evaluates it
+        if (dir == 0 && a.Dx[0]) {
 #pragma unroll
-        for (int n = 0; n < NQ; ++n) val[n] += c * (ld_stream(Hm[n], s - st) - ld_stream(a.H[dir][n], s));
+            for (int n = 0; n < NQ; ++n) val[n] += c * ld_stream(a.Dx[n], s);
+        } else {
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) val[n] += c * (ld_stream(Hm[n], s - st) - ld_stream(a.H[dir][n], s));
+        }
         if (Phys<PHYS>::PIMUNU) {
             double d[16];
             const double f = a.inv2h[dir];
